@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""FoF throughput on B200: Mparticles/s on the 256^3 periodic box (default).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one pass of the hot path (ingest + images, keys, sort, cells,
+befriending, groups, property sums, ownership, catalog) over the seeded
+synthetic 256^3 box (16.8M particles, L = 1000 Mpc/h, FP32 positions,
+10,000 Plummer clumps holding 60 % of the particles, linking parameter 0.2,
+Boundarysize 10).  The headline form is FP32 pair tests with FP64 re-check of
+the band; the plain FP64 form is measured on the same box and reported
+beside it.  With N GPUs (torchrun) every rank runs its own box (weak
+scaling; the boxes are independent domains, there is no exchange).
+
+Timing: CUDA events on the launching stream, W untimed warm-up steps, K timed
+steps between barriers + synchronize; inputs (400 MB) exceed L2.
+`e2e` repeats the measurement through the public API with pinned host
+inputs: host->device copy, the run, and the catalog read back.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "FoF Mparticles/s at 256^3: FP32+FP64-recheck vs plain; exact groups"
+UNIT = "Mparticles/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def make_workload(args, rank):
+    from cm_halofinder_b200 import synth
+    if args.config == "c2":
+        return synth.config2(seed=2 + rank, scale=args.scale)
+    if args.config == "c1":
+        return synth.config1(seed=1 + rank, scale=args.scale)
+    if args.config == "c5":
+        return synth.config5(seed=5 + rank, scale=args.scale)
+    raise SystemExit(f"unknown config {args.config}")
+
+
+def stage_bytes(st, pos_bytes):
+    """Algorithmic bytes per stage (the minimum data each stage must move in
+    this design): see the measurement section of the design notes."""
+    n, npr, R = st["n_in"], st["n_proc"], st["n_cells"]
+    passes = (st["key_bits"] + 7) // 8
+    rec = 16 if pos_bytes == 4 else 32
+    return {
+        "ingest": 2 * 3 * pos_bytes * n + npr * (8 + 4 + rec),
+        "sort": passes * npr * 2 * (8 + 4),
+        "cells": npr * (4 + rec + rec + 8 + 4) + R * 12,
+        "befriend": npr * rec + R * (8 + 4 + 4),
+        "groups": npr * (4 + 4 + 4) + R * 12,
+        "sums": npr * (4 + 4 + rec + 12),
+    }
+
+
+def run_ours(args):
+    import torch
+    from cm_halofinder_b200 import FofConfig, Plan
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    w = make_workload(args, rank)
+    n = w.n
+    dev = torch.device("cuda", local)
+    pos = torch.from_numpy(w.pos).to(dev)
+    vel = torch.from_numpy(w.vel).to(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(plan, steps, warmup):
+        for _ in range(warmup):
+            plan.run(pos, vel, out="device", stream=stream)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        stages = {}
+        launches = 0
+        e0.record(stream)
+        for _ in range(steps):
+            cat = plan.run(pos, vel, out="device", stream=stream)
+            st = cat.stats.as_dict()
+            launches += st["n_launches"]
+            for k, v in st["stage_ms"].items():
+                stages[k] = stages.get(k, 0.0) + v / steps
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, st, stages, launches
+
+    cfg_fast = FofConfig.from_workload(w, precision=args.precision)
+    plan = Plan(cfg_fast, pos_dtype=w.pos.dtype, device=local)
+    clocks = ClockSampler(local)
+    for _ in range(args.warmup):
+        plan.run(pos, vel, out="device", stream=stream)
+    clocks.start()
+    ms, st, stages, launches = timed(plan, args.steps, 0)
+    clk = clocks.stop()
+    value = n * world / (ms * 1e-3) / 1e6
+
+    plain = None
+    if not args.no_plain and args.precision != "fp64":
+        plan_p = Plan(FofConfig.from_workload(w, precision="fp64"), pos_dtype=w.pos.dtype,
+                      device=local)
+        ms_p, st_p, stages_p, _ = timed(plan_p, max(1, args.steps), args.warmup)
+        plain = {"value": n * world / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
+                 "n_pair_tests": st_p["n_pair_tests"],
+                 "stage_ms": {k: round(v, 4) for k, v in stages_p.items()},
+                 "speedup_of_chosen_form": ms_p / ms}
+        plan_p.close()
+
+    # end to end through the public API: pinned host inputs, catalog back
+    pin_pos = torch.from_numpy(w.pos).pin_memory().numpy()
+    pin_vel = torch.from_numpy(w.vel).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        plan.run(pin_pos, pin_vel, out="host", stream=stream)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    d2h = 0
+    for _ in range(args.steps):
+        hc = plan.run(pin_pos, pin_vel, out="host", stream=stream)
+        d2h = hc.props.nbytes + hc.head.nbytes
+    e1.record(stream)
+    barrier()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": n * world / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": int(w.pos.nbytes + w.vel.nbytes), "d2h_bytes_per_step": int(d2h)}
+
+    peak, peak_kind = peaks()
+    pos_bytes = w.pos.dtype.itemsize
+    sb = stage_bytes(st, pos_bytes)
+    dominant = max(sb, key=lambda k: stages.get(k, 0.0))
+    ach = sb[dominant] / (stages[dominant] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": args.traffic,
+                "algorithmic_bytes_per_launch": int(sb[dominant]),
+                "stage_gbs": {k: round(sb[k] / (stages[k] * 1e-3) / 1e9, 1)
+                              for k in sb if stages.get(k, 0) > 0}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, args.cpu_seconds)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64-recheck" if args.precision == "fp32" else "f64",
+        "data": "synthetic (seeded Plummer clumps + uniform background)",
+        "config": {"workload": f"{args.config}: periodic box L={w.hi[0]:.1f} Mpc/h, "
+                               f"N={n}, FP32 positions, {w.meta['n_clumps']} clumps, "
+                               f"l={w.linklength:.6f}, Boundarysize={w.boundary}",
+                   "n_particles": n, "n_processed": st["n_proc"], "n_images": st["n_images"],
+                   "n_halos": st["nhalos"], "n_groups": st["n_groups"],
+                   "n_fine_cells": st["n_cells"], "cell_factor": st["cell_factor"],
+                   "pair_tests": st["n_pair_tests"], "rechecks": st["n_rechecks"],
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "inputs (400 MB) larger than L2; no flush"},
+        "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "plain_fp64": plain,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(w, seconds, ndiv=16, timeout=None, procs=1, seed=0):
+    """The reference's own FoF (oracle/_ref) on host cores, on sub-boxes of
+    the same box (one rank's domain of an ndiv^3 decomposition each)."""
+    from oracle import reference
+    if not reference.available("cmh_ref_f32_timing"):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "reference binary not built (oracle/_ref missing)"}
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(ndiv ** 3)
+    timeout = timeout or max(5.0, seconds / 2)
+    done_n, spent, ok, to = 0, 0.0, 0, 0
+    t_end = time.perf_counter() + seconds
+    k = 0
+    while time.perf_counter() < t_end and k < len(order):
+        sb = reference.SubBox(w, ndiv, int(order[k]))
+        k += 1
+        dt, wall = reference.time_subbox(sb, timeout=min(timeout, max(1.0, t_end - time.perf_counter() + 1)))
+        spent += wall
+        if dt is None:
+            to += 1
+        else:
+            ok += 1
+            done_n += sb.n_owned
+    value = done_n / spent / 1e6 if spent > 0 else None
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{ok} of {ndiv}^3 sub-box domains (one rank each, ghost shell "
+                      f"{w.boundary}) of this box run to completion, {to} stopped at the "
+                      f"per-domain time limit and counted with zero particles; "
+                      f"{spent:.1f} s of one core"}
+
+
+def _ref_worker(argv):
+    from oracle import reference
+    w_args, index, ndiv, timeout = argv
+    import pickle
+    w = pickle.loads(w_args)
+    sb = reference.SubBox(w, ndiv, index)
+    dt, wall = reference.time_subbox(sb, timeout=timeout)
+    return (sb.n_owned if dt is not None else 0), wall, dt is None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from oracle import reference
+    if not reference.available("cmh_ref_f32_timing"):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference binaries (oracle/_ref) were not built"}))
+        return
+    import multiprocessing as mp
+    import pickle
+    w = make_workload(args, 0)
+    cores = os.cpu_count() or 1
+    ndiv = 16
+    order = np.random.default_rng(0).permutation(ndiv ** 3)
+    blob = pickle.dumps(w)
+    ctx = mp.get_context("spawn")
+    per_step = cores
+    timeout = args.ref_timeout
+    res = []
+    k = 0
+    with ctx.Pool(cores) as pool:
+        for step in range(args.warmup + args.steps):
+            jobs = [(blob, int(order[(k + j) % len(order)]), ndiv, timeout) for j in range(per_step)]
+            k += per_step
+            t0 = time.perf_counter()
+            out = pool.map(_ref_worker, jobs)
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                res.append((sum(o[0] for o in out), dt, sum(o[2] for o in out)))
+    nsum = sum(r[0] for r in res)
+    tsum = sum(r[1] for r in res)
+    tos = sum(r[2] for r in res)
+    value = nsum / tsum / 1e6
+    ms = tsum / len(res) * 1e3
+    sample = (f"each step: {per_step} sub-box domains of a {ndiv}^3 decomposition of the "
+              f"box, one reference process per core; {tos} of {per_step * len(res)} domains "
+              f"hit the {timeout:.0f} s limit and count zero particles")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"{args.config} (sampled sub-domains)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-timeout", type=float, default=20.0)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="dram bytes of the dominant kernel from an ncu capture")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,287 @@
+"""B200 Friends-of-Friends halo finder: drop-in for CM_Halofinder's FoF path.
+
+Python face of the C ABI in include/cmh_fof.h.  The compute runs in the
+native library (cm_halofinder_b200/libcmh_fof.so, hand-written sm_100a
+kernels); there is no CPU fallback: importing works without a GPU, running
+FoF without one raises ``CmhError(CMH_ERR_NO_DEVICE)``.
+
+Reference interface mirrored here:
+* ``read_parameterfile``  <- Read_Parameterfile (src_v2/startup.c:109-314)
+* ``fof`` / ``Plan.run``  <- FOF() (src_v2/FOF.c:23-339): cell grid,
+  befriending, halo retrieval, Checkhalo ownership and the property sums of
+  Output_Halos; ``Catalog`` holds the unformatted halo records
+  (FOF.c:836-872) in head order
+* ``write_halos`` / ``write_info`` <- Output_Halos / Output_Info
+  (FOF.c:546-957)
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import (CMH_DEVICE, CMH_FLOAT32, CMH_FLOAT64, CMH_FP32_RECHECK, CMH_HOST,
+                   CMH_OUT_PARTICLE_ID, CMH_OUT_PARTICLES, CMH_OUT_UNFORMATTED,
+                   CMH_PLAIN_FP64, CMH_PROP_DISPERSION, CMH_PROP_INERTIA, CmhError)
+
+__all__ = [
+    "fof", "Plan", "Catalog", "FofConfig", "read_parameterfile", "write_halos", "write_info",
+    "CmhError", "CMH_FP32_RECHECK", "CMH_PLAIN_FP64", "CMH_PROP_INERTIA", "CMH_PROP_DISPERSION",
+    "CMH_OUT_UNFORMATTED", "CMH_OUT_PARTICLES", "CMH_OUT_PARTICLE_ID", "halosize",
+]
+
+PRECISION = {"fp64": CMH_PLAIN_FP64, "plain": CMH_PLAIN_FP64, "fp32": CMH_FP32_RECHECK,
+             "fp32_recheck": CMH_FP32_RECHECK}
+
+
+def halosize(properties=0):
+    """Floats per halo record (FOF.c:574-580)."""
+    return 7 + (6 if properties & 1 else 0) + (6 if properties & 2 else 0)
+
+
+@dataclass
+class FofConfig:
+    """The run parameters FOF() reads, for one domain (Nx = Ny = Nz = 1)."""
+
+    lo: tuple
+    hi: tuple
+    boundary: float
+    linklength: float
+    nphalomin: float = 10.0
+    periodic: bool = True
+    precision: str = "fp32"
+    properties: int = 0
+    cell_factor: int = 0
+    varlink: dict | None = None       # {"origin", "rmax", "table", "ref_cells"}
+
+    def to_c(self):
+        p = _abi.FofParams()
+        for a in range(3):
+            p.lo[a] = float(self.lo[a])
+            p.hi[a] = float(self.hi[a])
+        p.boundary = float(self.boundary)
+        p.linklength = float(self.linklength)
+        p.nphalomin = float(self.nphalomin)
+        p.periodic = int(bool(self.periodic))
+        p.precision = PRECISION[self.precision] if isinstance(self.precision, str) \
+            else int(self.precision)
+        p.properties = int(self.properties)
+        p.cell_factor = int(self.cell_factor)
+        p.varlink = 0
+        if self.varlink:
+            tab = np.ascontiguousarray(self.varlink["table"], np.float64)
+            p._keep = tab
+            p.varlink = 1
+            rc = self.varlink.get("ref_cells", (1, 1, 1))
+            if np.isscalar(rc):
+                rc = (rc, rc, rc)
+            for a in range(3):
+                p.origin[a] = float(self.varlink["origin"][a])
+                p.ref_cells[a] = int(rc[a])
+            p.ltab_n = len(tab)
+            p.ltab_rmax = float(self.varlink["rmax"])
+            p.ltab = tab.ctypes.data_as(C.POINTER(C.c_double))
+        return p
+
+    @classmethod
+    def from_workload(cls, w, precision="fp32", properties=0, cell_factor=0):
+        vl = None
+        if getattr(w, "varlink", None):
+            vl = dict(w.varlink)
+            vl["ref_cells"] = w.cells
+        return cls(lo=w.lo, hi=w.hi, boundary=w.boundary, linklength=w.linklength,
+                   nphalomin=w.nphalomin, periodic=w.periodic, precision=precision,
+                   properties=properties, cell_factor=cell_factor, varlink=vl)
+
+
+@dataclass
+class Catalog:
+    """Owned halos in head order: ``props[h]`` is the reference's unformatted
+    record (n, x, y, z, vx, vy, vz [, inertia] [, dispersion])."""
+
+    props: np.ndarray
+    head: np.ndarray
+    member: np.ndarray | None
+    stats: dict
+
+    @property
+    def nhalos(self):
+        return int(self.props.shape[0])
+
+
+def _dtype_code(a):
+    if a.dtype == np.float32:
+        return CMH_FLOAT32
+    if a.dtype == np.float64:
+        return CMH_FLOAT64
+    raise TypeError("positions and velocities must be float32 or float64")
+
+
+def _host_catalog(cat):
+    nh, hs = int(cat.nhalos), int(cat.halosize)
+    props = np.ctypeslib.as_array(cat.props, shape=(max(nh, 1), hs))[:nh].copy() \
+        if nh else np.zeros((0, hs), np.float32)
+    head = np.ctypeslib.as_array(cat.head, shape=(max(nh, 1),))[:nh].copy() \
+        if nh else np.zeros(0, np.uint32)
+    member = None
+    if bool(cat.member):
+        n = int(cat.stats.n_in)
+        member = np.ctypeslib.as_array(cat.member, shape=(max(n, 1),))[:n].copy()
+    return Catalog(props=props, head=head, member=member, stats=cat.stats.as_dict())
+
+
+def fof(pos, vel, config: FofConfig, ids=None, members=False, stream=None):
+    """One-shot FoF on host (numpy) arrays; returns a host Catalog.
+
+    Equivalent of the reference's FOF() for one domain, minus the file
+    writers (see write_halos)."""
+    L = _abi.lib()
+    pos = np.ascontiguousarray(pos)
+    vel = np.ascontiguousarray(vel)
+    if pos.ndim != 2 or pos.shape[1] != 3 or vel.shape != pos.shape:
+        raise ValueError("pos and vel must be (N, 3)")
+    parts = _abi.Particles(n=pos.shape[0], pos_dtype=_dtype_code(pos), vel_dtype=_dtype_code(vel),
+                           pos=pos.ctypes.data, vel=vel.ctypes.data,
+                           id=None if ids is None else np.ascontiguousarray(ids, np.uint64).ctypes.data,
+                           location=CMH_HOST)
+    p = config.to_c()
+    cat = _abi.Catalog()
+    _abi.check(L.cmh_fof_run(C.byref(p), C.byref(parts), C.byref(cat), int(members),
+                             C.c_void_p(stream or 0)))
+    try:
+        return _host_catalog(cat)
+    finally:
+        L.cmh_catalog_free(C.byref(cat))
+
+
+class Plan:
+    """Device-resident repeated runs (cmh_plan_*).  Particles are torch CUDA
+    tensors (N, 3) or raw device pointers with explicit dtypes."""
+
+    def __init__(self, config: FofConfig, pos_dtype=np.float32, device=0, max_particles=0):
+        self._L = _abi.lib()
+        self.config = config
+        self._p = config.to_c()
+        h = C.c_void_p()
+        _abi.check(self._L.cmh_plan_create(C.byref(h), C.byref(self._p), int(max_particles),
+                                           CMH_FLOAT64 if np.dtype(pos_dtype) == np.float64
+                                           else CMH_FLOAT32, int(device)))
+        self._h = h
+
+    def set_config(self, config: FofConfig):
+        self.config = config
+        self._p = config.to_c()
+        _abi.check(self._L.cmh_plan_set_params(self._h, C.byref(self._p)))
+
+    @staticmethod
+    def _ptr(t):
+        return int(t.data_ptr()) if hasattr(t, "data_ptr") else int(t)
+
+    @staticmethod
+    def _tdt(t):
+        s = str(getattr(t, "dtype", ""))
+        return CMH_FLOAT64 if "float64" in s else CMH_FLOAT32
+
+    def run(self, pos, vel, n=None, members=False, out="host", stream=None,
+            pos_dtype=None, vel_dtype=None):
+        """Run on torch CUDA tensors (device-resident) or numpy arrays (host;
+        copied to the device on `stream` inside the call)."""
+        n = int(pos.shape[0]) if n is None else int(n)
+        if isinstance(pos, np.ndarray):
+            if not (pos.flags.c_contiguous and vel.flags.c_contiguous):
+                raise ValueError("host arrays must be C-contiguous")
+            parts = _abi.Particles(n=n, pos_dtype=_dtype_code(pos), vel_dtype=_dtype_code(vel),
+                                   pos=pos.ctypes.data, vel=vel.ctypes.data, id=None,
+                                   location=CMH_HOST)
+        else:
+            parts = _abi.Particles(n=n,
+                                   pos_dtype=self._tdt(pos) if pos_dtype is None else pos_dtype,
+                                   vel_dtype=self._tdt(vel) if vel_dtype is None else vel_dtype,
+                                   pos=self._ptr(pos), vel=self._ptr(vel), id=None,
+                                   location=CMH_DEVICE)
+        cat = _abi.Catalog()
+        loc = CMH_HOST if out == "host" else CMH_DEVICE
+        if stream is None:
+            sp = 0
+        elif hasattr(stream, "cuda_stream"):
+            sp = stream.cuda_stream
+        else:
+            sp = int(stream)
+        _abi.check(self._L.cmh_plan_run(self._h, C.byref(parts), C.byref(cat), int(members),
+                                        loc, C.c_void_p(sp)))
+        if loc == CMH_DEVICE:
+            return cat  # raw struct: device pointers into plan-owned memory
+        try:
+            return _host_catalog(cat)
+        finally:
+            self._L.cmh_catalog_free(C.byref(cat))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cmh_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_parameterfile(fname, varlink=False):
+    """Read a run_parameters file with the reference's rules
+    (startup.c:109-314); raises CmhError(CMH_ERR_PARAMETER_FILE) on a
+    missing, unknown or repeated tag."""
+    rp = _abi.RunParameters()
+    _abi.check(_abi.lib().cmh_read_parameterfile(str(fname).encode(), int(varlink),
+                                                  C.byref(rp)))
+    return rp
+
+
+def config_from_run(rp, task=0, periodic=False, precision="fp32", properties=0):
+    """FoF parameters of one task's domain (Set_Params, startup.c:33-47)."""
+    p = _abi.FofParams()
+    _abi.check(_abi.lib().cmh_params_from_run(C.byref(rp), int(task), int(periodic), C.byref(p)))
+    return FofConfig(lo=tuple(p.lo), hi=tuple(p.hi), boundary=p.boundary,
+                     linklength=p.linklength, nphalomin=p.nphalomin, periodic=bool(p.periodic),
+                     precision=precision, properties=properties)
+
+
+def write_halos(base, task, catalog: Catalog, pos=None, vel=None, ids=None, flags=0):
+    """Write "<base>.<task>" in the reference's Output_Halos layout."""
+    L = _abi.lib()
+    nh, hs = catalog.props.shape
+    props = np.ascontiguousarray(catalog.props, np.float32)
+    head = np.ascontiguousarray(catalog.head, np.uint32)
+    cat = _abi.Catalog(nhalos=nh, halosize=hs, location=CMH_HOST,
+                       props=props.ctypes.data_as(C.POINTER(C.c_float)),
+                       head=head.ctypes.data_as(C.POINTER(C.c_uint32)))
+    keep = [props, head]
+    parts = None
+    if catalog.member is not None:
+        mem = np.ascontiguousarray(catalog.member, np.int64)
+        keep.append(mem)
+        cat.member = mem.ctypes.data_as(C.POINTER(C.c_int64))
+        cat.stats.n_in = mem.shape[0]
+    if pos is not None:
+        pos = np.ascontiguousarray(pos)
+        vel = np.ascontiguousarray(vel)
+        idp = None
+        if ids is not None:
+            ids = np.ascontiguousarray(ids, np.uint64)
+            idp = ids.ctypes.data
+        keep += [pos, vel, ids]
+        parts = _abi.Particles(n=pos.shape[0], pos_dtype=_dtype_code(pos),
+                               vel_dtype=_dtype_code(vel), pos=pos.ctypes.data,
+                               vel=vel.ctypes.data, id=idp, location=CMH_HOST)
+    _abi.check(L.cmh_write_halos(str(base).encode(), int(task), C.byref(cat),
+                                 C.byref(parts) if parts is not None else None, int(flags)))
+
+
+def write_info(base, rp, nhalos_per_task):
+    L = _abi.lib()
+    arr = np.ascontiguousarray(nhalos_per_task, np.int64)
+    _abi.check(L.cmh_write_info(str(base).encode(), C.byref(rp),
+                                arr.ctypes.data_as(C.POINTER(C.c_int64)), len(arr)))

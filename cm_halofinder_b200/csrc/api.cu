@@ -1,0 +1,337 @@
+// C ABI of the FoF library (include/cmh_fof.h): plans, one-shot runs,
+// catalogs, errors.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "cmh_internal.cuh"
+#include "plan.cuh"
+
+namespace cmh {
+
+thread_local long long g_launches = 0;
+
+namespace {
+thread_local std::string g_last_error;
+
+struct CatalogStore {
+  bool host_owned = false;
+};
+}  // namespace
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
+  if (e == cudaSuccess) return;
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  throw Error{e == cudaErrorMemoryAllocation ? CMH_ERR_OUT_OF_MEMORY : CMH_ERR_CUDA, buf};
+}
+
+void fail(cmh_status code, const std::string &msg) { throw Error{code, msg}; }
+
+void DevBuf::ensure(size_t bytes) {
+  if (bytes <= cap && p) return;
+  if (p) CMH_CUDA(cudaFree(p));
+  p = nullptr;
+  cap = 0;
+  size_t want = bytes + bytes / 8 + 256;  // headroom against small regrowth
+  CMH_CUDA(cudaMalloc(&p, want));
+  cap = want;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+}
+
+Plan::Plan(const cmh_fof_params &p, int pdt, int dev) : device(dev), pos_dtype(pdt) {
+  CMH_CUDA(cudaSetDevice(device));
+  int major = 0;
+  CMH_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major < 10) fail(CMH_ERR_NO_DEVICE, "the FoF kernels are built for sm_100a (B200)");
+  CMH_CUDA(cudaMallocHost(&h_scal, 64 * sizeof(uint32_t)));
+  CMH_CUDA(cudaEventCreate(&ev0));
+  CMH_CUDA(cudaEventCreate(&ev1));
+  for (cudaEvent_t &e : stage_ev) CMH_CUDA(cudaEventCreate(&e));
+  set_params(p);
+}
+
+Plan::~Plan() {
+  cudaSetDevice(device);
+  DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_keep, &b_nimg,
+                   &b_keep_scan, &b_img_scan, &b_keys, &b_keys_alt, &b_vals, &b_vals_alt,
+                   &b_ppos, &b_spos, &b_run_of, &b_run_start, &b_run_g, &b_top_first,
+                   &b_top_end, &b_top_slot, &b_rtmp1, &b_rtmp2, &b_maps, &b_parent, &b_count,
+                   &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
+                   &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
+                   &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
+                   &in_pos, &in_vel};
+  for (DevBuf *b : all) b->release();
+  if (h_scal) cudaFreeHost(h_scal);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  for (cudaEvent_t e : stage_ev)
+    if (e) cudaEventDestroy(e);
+}
+
+void Plan::set_params(const cmh_fof_params &p) {
+  if (!(p.linklength > 0) || !(p.boundary >= 0))
+    fail(CMH_ERR_INVALID_ARGUMENT, "Linklength must be > 0 and Boundarysize >= 0");
+  if (p.precision != CMH_PLAIN_FP64 && p.precision != CMH_FP32_RECHECK)
+    fail(CMH_ERR_INVALID_ARGUMENT, "unknown precision mode");
+  params = p;
+  fp32 = p.precision == CMH_FP32_RECHECK;
+  ltab_host.clear();
+  if (p.varlink) {
+    if (p.ltab_n < 2 || !p.ltab || !(p.ltab_rmax > 0))
+      fail(CMH_ERR_INVALID_ARGUMENT, "variable linking length needs a table of >= 2 entries");
+    ltab_host.assign(p.ltab, p.ltab + p.ltab_n);
+  }
+  params.ltab = nullptr;  // the plan keeps its own copy
+}
+
+}  // namespace cmh
+
+using cmh::Error;
+using cmh::Plan;
+
+#define CMH_API_BEGIN try {
+#define CMH_API_END                                 \
+  return CMH_OK;                                    \
+  }                                                 \
+  catch (const Error &e) {                          \
+    cmh::set_error(e.msg);                          \
+    return e.code;                                  \
+  }                                                 \
+  catch (const std::bad_alloc &) {                  \
+    cmh::set_error("host allocation failed");       \
+    return CMH_ERR_OUT_OF_MEMORY;                   \
+  }                                                 \
+  catch (const std::exception &e) {                 \
+    cmh::set_error(e.what());                       \
+    return CMH_ERR_INVALID_ARGUMENT;                \
+  }
+
+namespace {
+
+void check_parts(const cmh_particles *parts) {
+  if (!parts) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "particles is NULL");
+  if (parts->n < 0) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "negative particle count");
+  if (parts->n > 0 && (!parts->pos || !parts->vel))
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "pos and vel are required");
+  if ((parts->pos_dtype != CMH_FLOAT32 && parts->pos_dtype != CMH_FLOAT64) ||
+      (parts->vel_dtype != CMH_FLOAT32 && parts->vel_dtype != CMH_FLOAT64))
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "unknown dtype");
+  if (parts->n >= (int64_t)0xfffffff0ll)
+    cmh::fail(CMH_ERR_CAPACITY, "more than 2^32 particles in one domain");
+}
+
+// Copies the plan's last catalog to host arrays owned by `cat`.
+void catalog_to_host(Plan &pl, cmh_catalog *cat, bool want_member, int64_t n_in,
+                     cudaStream_t s) {
+  const int64_t nh = pl.out_nhalos;
+  const int hs = pl.geom.hs;
+  cat->nhalos = nh;
+  cat->halosize = hs;
+  cat->location = CMH_HOST;
+  cat->props = (float *)malloc(sizeof(float) * (size_t)std::max<int64_t>(nh * hs, 1));
+  cat->head = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)std::max<int64_t>(nh, 1));
+  cat->member = nullptr;
+  cat->member_proc = nullptr;
+  cat->member_pos = nullptr;
+  cat->impl = new cmh::CatalogStore{true};
+  if (want_member) {
+    const size_t nn = (size_t)std::max<int64_t>(n_in, 1);
+    cat->member = (int64_t *)malloc(sizeof(int64_t) * nn);
+    cat->member_proc = (uint32_t *)malloc(sizeof(uint32_t) * nn);
+    cat->member_pos = (float *)malloc(sizeof(float) * 3 * nn);
+  }
+  if (!cat->props || !cat->head ||
+      (want_member && (!cat->member || !cat->member_proc || !cat->member_pos)))
+    cmh::fail(CMH_ERR_OUT_OF_MEMORY, "host catalog allocation failed");
+  if (nh > 0) {
+    CMH_CUDA(cudaMemcpyAsync(cat->props, pl.b_props.p, sizeof(float) * nh * hs,
+                             cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->head, pl.b_head_out.p, sizeof(uint32_t) * nh,
+                             cudaMemcpyDeviceToHost, s));
+  }
+  if (want_member && n_in > 0) {
+    CMH_CUDA(cudaMemcpyAsync(cat->member, pl.b_member.p, sizeof(int64_t) * n_in,
+                             cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->member_proc, pl.b_member_proc.p, sizeof(uint32_t) * n_in,
+                             cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->member_pos, pl.b_member_pos.p, sizeof(float) * 3 * n_in,
+                             cudaMemcpyDeviceToHost, s));
+  }
+  CMH_CUDA(cudaStreamSynchronize(s));
+  cat->stats = pl.stats;
+}
+
+void catalog_on_device(Plan &pl, cmh_catalog *cat, bool want_member) {
+  cat->nhalos = pl.out_nhalos;
+  cat->halosize = pl.geom.hs;
+  cat->location = CMH_DEVICE;
+  cat->props = pl.b_props.as<float>();
+  cat->head = pl.b_head_out.as<uint32_t>();
+  cat->member = want_member ? pl.b_member.as<int64_t>() : nullptr;
+  cat->member_proc = want_member ? pl.b_member_proc.as<uint32_t>() : nullptr;
+  cat->member_pos = want_member ? pl.b_member_pos.as<float>() : nullptr;
+  cat->impl = nullptr;
+  cat->stats = pl.stats;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cmh_abi_version(void) { return CMH_ABI_VERSION; }
+
+size_t cmh_last_error(char *buf, size_t len) {
+  const std::string &m = cmh::g_last_error;
+  if (buf && len) {
+    size_t k = m.size() < len - 1 ? m.size() : len - 1;
+    memcpy(buf, m.data(), k);
+    buf[k] = 0;
+  }
+  return m.size();
+}
+
+cmh_status cmh_plan_create(cmh_plan **plan, const cmh_fof_params *params,
+                           int64_t max_particles, int32_t pos_dtype, int32_t device) {
+  CMH_API_BEGIN
+  if (!plan || !params) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and params are required");
+  *plan = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    cmh::fail(CMH_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "bad device index");
+  (void)max_particles;
+  *plan = new Plan(*params, pos_dtype, device);
+  CMH_API_END
+}
+
+cmh_status cmh_plan_set_params(cmh_plan *plan, const cmh_fof_params *params) {
+  CMH_API_BEGIN
+  if (!plan || !params) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and params are required");
+  static_cast<Plan *>(plan)->set_params(*params);
+  CMH_API_END
+}
+
+cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog *cat,
+                        int32_t want_member, int32_t out_location, void *stream) {
+  CMH_API_BEGIN
+  if (!plan || !cat) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and catalog are required");
+  check_parts(parts);
+  Plan &pl = *static_cast<Plan *>(plan);
+  if (parts->pos_dtype != pl.pos_dtype)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "position dtype differs from the plan's");
+  memset(cat, 0, sizeof *cat);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cmh_particles dp = *parts;
+  if (parts->location == CMH_HOST && parts->n > 0) {
+    // host particles: copied into plan-owned device buffers on the stream
+    CMH_CUDA(cudaSetDevice(pl.device));
+    const size_t pb = (size_t)parts->n * 3 * (parts->pos_dtype == CMH_FLOAT64 ? 8 : 4);
+    const size_t vb = (size_t)parts->n * 3 * (parts->vel_dtype == CMH_FLOAT64 ? 8 : 4);
+    pl.in_pos.ensure(pb);
+    pl.in_vel.ensure(vb);
+    CMH_CUDA(cudaMemcpyAsync(pl.in_pos.p, parts->pos, pb, cudaMemcpyHostToDevice, s));
+    CMH_CUDA(cudaMemcpyAsync(pl.in_vel.p, parts->vel, vb, cudaMemcpyHostToDevice, s));
+    dp.pos = pl.in_pos.p;
+    dp.vel = pl.in_vel.p;
+    dp.location = CMH_DEVICE;
+  }
+  pl.run(dp, want_member != 0, s);
+  if (out_location == CMH_DEVICE) catalog_on_device(pl, cat, want_member != 0);
+  else catalog_to_host(pl, cat, want_member != 0, parts->n, s);
+  CMH_API_END
+}
+
+void cmh_plan_destroy(cmh_plan *plan) { delete static_cast<Plan *>(plan); }
+
+void cmh_catalog_free(cmh_catalog *cat) {
+  if (!cat) return;
+  auto *st = static_cast<cmh::CatalogStore *>(cat->impl);
+  if (st && st->host_owned) {
+    free(cat->props);
+    free(cat->head);
+    free(cat->member);
+    free(cat->member_proc);
+    free(cat->member_pos);
+  }
+  delete st;
+  cat->props = nullptr;
+  cat->head = nullptr;
+  cat->member = nullptr;
+  cat->member_proc = nullptr;
+  cat->member_pos = nullptr;
+  cat->impl = nullptr;
+  cat->nhalos = 0;
+}
+
+cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
+                       cmh_catalog *cat, int32_t want_member, void *stream) {
+  CMH_API_BEGIN
+  if (!params || !cat) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "params and catalog are required");
+  check_parts(parts);
+  memset(cat, 0, sizeof *cat);
+  int dev = 0;
+  CMH_CUDA(cudaGetDevice(&dev));
+  std::unique_ptr<Plan> pl(new Plan(*params, parts->pos_dtype, dev));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cmh_particles dp = *parts;
+  cmh::DevBuf dpos, dvel;
+  if (parts->location == CMH_HOST && parts->n > 0) {
+    const size_t pb = (size_t)parts->n * 3 * (parts->pos_dtype == CMH_FLOAT64 ? 8 : 4);
+    const size_t vb = (size_t)parts->n * 3 * (parts->vel_dtype == CMH_FLOAT64 ? 8 : 4);
+    dpos.ensure(pb);
+    dvel.ensure(vb);
+    CMH_CUDA(cudaMemcpyAsync(dpos.p, parts->pos, pb, cudaMemcpyHostToDevice, s));
+    CMH_CUDA(cudaMemcpyAsync(dvel.p, parts->vel, vb, cudaMemcpyHostToDevice, s));
+    dp.pos = dpos.p;
+    dp.vel = dvel.p;
+    dp.location = CMH_DEVICE;
+  }
+  try {
+    pl->run(dp, want_member != 0, s);
+    catalog_to_host(*pl, cat, want_member != 0, parts->n, s);
+  } catch (...) {
+    dpos.release();
+    dvel.release();
+    throw;
+  }
+  dpos.release();
+  dvel.release();
+  CMH_API_END
+}
+
+cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *parts,
+                             int32_t nbox, cmh_catalog *cats, void *stream) {
+  CMH_API_BEGIN
+  if (!params || !parts || !cats || nbox < 0)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "params, particles and catalogs are required");
+  for (int b = 0; b < nbox; b++) memset(&cats[b], 0, sizeof cats[b]);
+  if (nbox == 0) return CMH_OK;
+  int dev = 0;
+  CMH_CUDA(cudaGetDevice(&dev));
+  std::unique_ptr<Plan> pl(new Plan(params[0], parts[0].pos_dtype, dev));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int b = 0; b < nbox; b++) {
+    check_parts(&parts[b]);
+    if (parts[b].location != CMH_DEVICE)
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "batched runs take device-resident particles");
+    pl->set_params(params[b]);
+    pl->pos_dtype = parts[b].pos_dtype;
+    pl->run(parts[b], false, s);
+    catalog_to_host(*pl, &cats[b], false, parts[b].n, s);
+  }
+  CMH_API_END
+}
+
+}  // extern "C"

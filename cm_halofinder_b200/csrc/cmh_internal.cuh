@@ -1,0 +1,72 @@
+// Internal declarations of the B200 FoF library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/cmh_fof.h"
+
+namespace cmh {
+
+constexpr int kSMs = 148;  // B200: 2 dies x 74 SMs
+
+// Per-thread error message behind cmh_last_error().
+void set_error(const std::string &msg);
+
+struct Error {
+  cmh_status code;
+  std::string msg;
+};
+
+// Throws Error on a CUDA failure; the C ABI layer turns it into a status.
+void cuda_check(cudaError_t e, const char *what, const char *file, int line);
+#define CMH_CUDA(x) ::cmh::cuda_check((x), #x, __FILE__, __LINE__)
+
+// Kernels launched by this host thread (reported per run in cmh_stats).
+extern thread_local long long g_launches;
+#define CMH_LAUNCHED()                     \
+  do {                                     \
+    CMH_CUDA(cudaGetLastError());          \
+    ++::cmh::g_launches;                   \
+  } while (0)
+[[noreturn]] void fail(cmh_status code, const std::string &msg);
+
+// Grid size for a grid-stride kernel: a multiple of the SM count, capped by
+// the work.
+inline unsigned grid_for(int64_t n, int threads, int per_sm = 8) {
+  int64_t want = (n + threads - 1) / threads;
+  int64_t cap = (int64_t)kSMs * per_sm;
+  if (want < 1) want = 1;
+  return (unsigned)(want < cap ? want : cap);
+}
+
+// Growable device buffer.
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t bytes);
+  void release();
+  template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// ---- scan.cu ---------------------------------------------------------------
+// Exclusive prefix sum of n uint32 values; `total` (device, may be null)
+// receives the sum.  Scratch is taken from `tmp` (grown as needed).
+void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n,
+                        uint32_t *total, DevBuf &tmp, cudaStream_t s);
+
+// ---- radix_sort.cu -----------------------------------------------------------
+// Stable LSD radix sort of (key u64, value u32) pairs on the low `bits` key
+// bits.  Result lands in keys/vals (the alt buffers are scratch); `tmp`
+// holds the digit count tables and `scan_tmp` the scratch of their scan.
+void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
+                        uint32_t *vals_alt, int64_t n, int bits, DevBuf &tmp,
+                        DevBuf &scan_tmp, cudaStream_t s);
+// Same for 32-bit keys.
+void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
+                        uint32_t *vals_alt, int64_t n, int bits, DevBuf &tmp,
+                        DevBuf &scan_tmp, cudaStream_t s);
+
+}  // namespace cmh

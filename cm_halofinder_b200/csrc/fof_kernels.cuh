@@ -1,0 +1,126 @@
+// Device-side geometry, pair predicates and union-find of the FoF pipeline.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cmh {
+
+// Particle position in cell order with the index of its source particle.
+template <class PT> struct SPos;
+template <> struct __align__(16) SPos<float> {
+  float x, y, z;
+  uint32_t src;
+};
+template <> struct __align__(16) SPos<double> {
+  double x, y, z;
+  uint32_t src, pad;
+};
+
+// Geometry and run parameters of one domain, passed by value to kernels.
+struct Geom {
+  double lo[3], hi[3];   // Lmin, Lmax
+  double rmin[3];        // lo - boundary (grid origin, rmin_buff)
+  double rmax[3];        // hi + boundary (rmax_buff)
+  double L[3];           // hi - lo
+  double boundary;
+  double linksq;         // Linklength^2 in double (FOF.c:60)
+  double maxlink;        // largest linking length (edge warning, pruning)
+  double prune_sq;       // (maxlink * (1 + 1e-5))^2: pairs of cells farther apart never link
+  double h;              // fine cell side, <= minimum linking length / sqrt(3)
+  double nphalomin;
+  float t_lo, t_hi;      // FP32 band: d2 < t_lo links, d2 > t_hi does not
+  int periodic;
+  int k;                 // fine cells per top-cell edge
+  int W;                 // fine-cell reach: cells more than W apart never link
+  int G[3];              // fine cells per axis
+  int T[3];              // top cells per axis
+  uint64_t k3;           // k^3
+  int props;             // CMH_PROP_* bits
+  int hs;                // floats per halo record
+  // variable linking length
+  int varlink;
+  double origin[3];
+  double ref_lcell[3];   // fixed grid of the l(r) rule
+  int ref_nc[3];
+  int ltab_n;
+  double ltab_dr;
+  const double *ltab;    // device copy of the table
+};
+
+// Running counters of one run, in device memory.
+struct Counters {
+  unsigned long long pair_tests;
+  unsigned long long rechecks;
+  unsigned long long member_conflicts;
+  unsigned int uf_giveups;     // union loops that hit their iteration cap
+  unsigned int domain_errors;  // particles outside [rmin, rmax] after ingest
+};
+
+// FP32 band around l^2: returns the thresholds t_lo < fl32(l2) < t_hi such
+// that d2_32 < t_lo implies the double test links and d2_32 > t_hi implies
+// it does not (proof in fof.cu above band_thresholds()).
+__host__ __device__ inline void band_thresholds(double l2, int ulps, float *t_lo,
+                                                float *t_hi) {
+  float l2f = (float)l2;
+  int e;
+  frexp((double)l2f, &e);                       // l2f in [2^(e-1), 2^e)
+  double ulp = ldexp(1.0, e - 1 - 23);          // spacing of floats at l2f
+  double lo = (double)l2f - ulps * ulp;
+  double hi = (double)l2f + ulps * ulp;
+  // outward rounding to float keeps the band at least this wide
+  float flo = (float)lo, fhi = (float)hi;
+  if ((double)flo > lo) flo = nextafterf(flo, -INFINITY);
+  if ((double)fhi < hi) fhi = nextafterf(fhi, INFINITY);
+  *t_lo = flo;
+  *t_hi = fhi;
+}
+
+// Fine-cell index along one axis: floor((x - rmin) / h), in double.
+__device__ __forceinline__ int fine_index(double x, double rmin, double h, int G) {
+  double q = __ddiv_rn(__dsub_rn(x, rmin), h);
+  int g = (int)floor(q);
+  g = g < 0 ? 0 : g;
+  return g >= G ? G - 1 : g;
+}
+
+// ---- union-find over occupied fine cells (lock-free, hook to min root) ----
+//
+// parent[x] <= x always holds: a root is only ever hooked under a smaller
+// root (atomicCAS), and path halving only stores ancestors.  Chains are
+// therefore strictly decreasing and find() terminates; the final root of a
+// component is its smallest cell index.
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
+  while (true) {
+    uint32_t p = __ldcg(parent + x);
+    if (p == x) return x;
+    uint32_t gp = __ldcg(parent + p);
+    if (gp == p) return p;
+    __stcg(parent + x, gp);  // path halving: gp is an ancestor of x
+    x = gp;
+  }
+}
+
+constexpr int kUnionCap = 1 << 22;
+
+__device__ __forceinline__ void uf_union(uint32_t *parent, uint32_t a, uint32_t b,
+                                         Counters *ctr) {
+  for (int it = 0; it < kUnionCap; it++) {
+    a = uf_find(parent, a);
+    b = uf_find(parent, b);
+    if (a == b) return;
+    if (a < b) {
+      uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    // hook the larger root a under the smaller root b
+    uint32_t old = atomicCAS(parent + a, a, b);
+    if (old == a) return;
+    a = old;  // a was hooked meanwhile; retry from its new parent
+  }
+  atomicAdd(&ctr->uf_giveups, 1u);
+}
+
+}  // namespace cmh

@@ -1,0 +1,240 @@
+/* cmh_fof.h -- C ABI of the B200 Friends-of-Friends halo finder.
+ *
+ * Drop-in for the FoF hot path of CM_Halofinder (src_v2/FOF.c, src_v2/link.c).
+ * Plain C types only: pointers, sizes and enums.  Every entry point returns a
+ * cmh_status; nothing aborts the process (the reference's FatalError ->
+ * MPI_Abort, main.c:107-112, becomes a status code plus cmh_last_error()).
+ *
+ * Threading: a cmh_plan is used by one host thread at a time and issues all
+ * device work on the stream given to it.  cmh_last_error() is per thread.
+ */
+#ifndef CMH_FOF_H
+#define CMH_FOF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMH_ABI_VERSION 1
+
+typedef enum cmh_status {
+  CMH_OK = 0,
+  CMH_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad enum          */
+  CMH_ERR_PARAMETER_FILE = 2,   /* Read_Parameterfile failures, startup.c:286-306 */
+  CMH_ERR_CUDA = 3,             /* a CUDA runtime call failed                */
+  CMH_ERR_OUT_OF_MEMORY = 4,    /* device or host allocation failed          */
+  CMH_ERR_DOMAIN = 5,           /* particle outside the padded domain
+                                   (read_data.c:810-812)                      */
+  CMH_ERR_CAPACITY = 6,         /* beyond 32-bit indices, a plan's capacity,
+                                   or a fixed scratch area                   */
+  CMH_ERR_DEVICE_TIMEOUT = 7,   /* a bounded device loop gave up             */
+  CMH_ERR_IO = 8,               /* file could not be opened / written        */
+  CMH_ERR_NO_DEVICE = 9         /* no usable sm_100 device                   */
+} cmh_status;
+
+typedef enum cmh_dtype { CMH_FLOAT32 = 0, CMH_FLOAT64 = 1 } cmh_dtype;
+
+/* Pair-test arithmetic.  Both give the reference's membership exactly.
+ *   CMH_PLAIN_FP64   : every pair test is the reference's double expression
+ *                      ((dx*dx + dy*dy) + dz*dz) <= Linklength^2 (FOF.c:351-357)
+ *   CMH_FP32_RECHECK : the test runs in FP32; a pair whose FP32 d^2 lies within
+ *                      4 ulp (8 ulp for FP64 positions) of FP32(l^2) is
+ *                      re-tested with the double expression.                */
+typedef enum cmh_precision { CMH_PLAIN_FP64 = 0, CMH_FP32_RECHECK = 1 } cmh_precision;
+
+typedef enum cmh_location { CMH_HOST = 0, CMH_DEVICE = 1 } cmh_location;
+
+#define CMH_PROP_INERTIA 1u    /* -DINERTIA    (FOF.c:849-854) */
+#define CMH_PROP_DISPERSION 2u /* -DDISPERSION (FOF.c:856-861) */
+
+/* Run parameters of the hot path: the subset of the reference's globals that
+ * FOF() reads (vars.h:100-117), for one domain (Nx = Ny = Nz = 1). */
+typedef struct cmh_fof_params {
+  double lo[3];        /* Lxmin, Lymin, Lzmin                                 */
+  double hi[3];        /* Lxmax, Lymax, Lzmax                                 */
+  double boundary;     /* Boundarysize: ghost-shell width                     */
+  double linklength;   /* Linklength (upper bound of l(r) when varlink)       */
+  double nphalomin;    /* Nphalomin: groups with fewer members are dropped    */
+  int32_t periodic;    /* 1: images within `boundary` of the faces are added  */
+  int32_t precision;   /* cmh_precision                                       */
+  uint32_t properties; /* CMH_PROP_* bits                                     */
+  int32_t cell_factor; /* fine cells per top-cell edge, 0 = autotune          */
+  /* Variable linking length (link.c): the linking length of a pair is the
+   * value at the centre of the lower-index cell of a fixed grid of
+   * ref_cells[a] cells over [lo-b, hi+b] (the reference's lcell grid), read
+   * from a uniform table over r = |centre - origin| in [0, ltab_rmax].      */
+  int32_t varlink;
+  int32_t ref_cells[3];
+  double origin[3];
+  int32_t ltab_n;
+  double ltab_rmax;
+  const double *ltab;  /* host pointer, ltab_n entries                         */
+} cmh_fof_params;
+
+/* Caller-owned particles, the fields of struct part_data (vars.h:36-47) as
+ * interleaved arrays: pos[3*i + a], vel[3*i + a]. */
+typedef struct cmh_particles {
+  int64_t n;
+  int32_t pos_dtype;   /* cmh_dtype                                           */
+  int32_t vel_dtype;   /* cmh_dtype                                           */
+  const void *pos;
+  const void *vel;
+  const uint64_t *id;  /* optional (PARTICLE_ID), may be NULL                 */
+  int32_t location;    /* cmh_location of all three pointers                  */
+} cmh_particles;
+
+typedef struct cmh_stats {
+  int64_t n_in;            /* particles given                                 */
+  int64_t n_out;           /* dropped outside the domain (read_data.c:409-424) */
+  int64_t n_images;        /* periodic images added                           */
+  int64_t n_proc;          /* particles processed = kept + images             */
+  int64_t n_cells;         /* occupied fine cells                             */
+  int64_t n_groups;        /* FoF groups, singletons included                 */
+  int64_t n_candidates;    /* groups with at least Nphalomin members          */
+  int64_t nhalos;          /* candidates whose centre of mass is owned        */
+  int64_t n_edge_warn;     /* owned halos with a member within Linklength of
+                              the padded-domain edge (FOF.c:403-422)          */
+  int64_t n_pair_tests;    /* pair predicate evaluations                      */
+  int64_t n_rechecks;      /* FP64 re-tests of band pairs                     */
+  int64_t n_member_conflicts; /* particles found in two owned halos           */
+  int32_t cell_factor;     /* fine cells per top-cell edge used               */
+  int32_t key_bits;        /* significant bits of the sort key                */
+  float ms_total;          /* device time of the run (CUDA events)            */
+  float stage_ms[8];       /* ingest, sort, cells, befriend, groups, sums,
+                              catalog, members (CUDA events on the stream)    */
+  int32_t n_launches;      /* kernels launched by the run                     */
+} cmh_stats;
+
+/* Halo catalog in the layout of the reference's unformatted records
+ * (FOF.c:836-872): per halo `halosize` floats
+ *   n, x, y, z, vx, vy, vz [, Ixx Iyy Izz Ixy Ixz Iyz] [, sxx syy szz sxy sxz syz]
+ * in ascending order of the halo head, the lowest processing index of the
+ * group (FOF.c:296-298). */
+typedef struct cmh_catalog {
+  int64_t nhalos;
+  int32_t halosize;
+  int32_t location;    /* cmh_location of the arrays                          */
+  float *props;        /* nhalos * halosize                                   */
+  uint32_t *head;      /* nhalos: processing index of the head                */
+  int64_t *member;     /* n_in: owned-halo index of each particle (or of one
+                          of its images), -1 if none; NULL if not requested   */
+  uint32_t *member_proc; /* n_in: processing index of that member copy       */
+  float *member_pos;   /* n_in x 3: its coordinates as stored (an image's
+                          coordinates are the wrapped ones, as the reference
+                          writes them, FOF.c:719-724)                          */
+  cmh_stats stats;
+  void *impl;          /* library-owned storage                               */
+} cmh_catalog;
+
+typedef struct cmh_plan cmh_plan;
+
+/* ---- library ------------------------------------------------------------ */
+
+int cmh_abi_version(void);
+
+/* Message of the last failing call on this host thread. */
+size_t cmh_last_error(char *buf, size_t len);
+
+/* ---- one-shot run: replaces void FOF(void) (src_v2/FOF.c:23, vars.h:121) - */
+
+/* Runs FoF on one domain and fills `cat` (host arrays, freed by
+ * cmh_catalog_free).  Particles may be host or device resident.  `want_member`
+ * requests cat->member.  `stream` is a cudaStream_t (NULL: legacy stream).
+ * Replaces FOF() from the cell grid (FOF.c:45-92) through Checkhalo
+ * (FOF.c:378-430) and the property sums of Output_Halos (FOF.c:797-872);
+ * the writers are cmh_write_halos / cmh_write_info below. */
+cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
+                       cmh_catalog *cat, int32_t want_member, void *stream);
+
+/* Frees what cmh_fof_run / cmh_plan_run put in a catalog. */
+void cmh_catalog_free(cmh_catalog *cat);
+
+/* ---- plans: device-resident repeated runs (same FOF() replacement) ------ */
+
+/* Creates a plan for up to `max_particles` input particles of `pos_dtype`
+ * on CUDA device `device`.  Device workspace is allocated here and grown on
+ * demand by cmh_plan_run. */
+cmh_status cmh_plan_create(cmh_plan **plan, const cmh_fof_params *params,
+                           int64_t max_particles, int32_t pos_dtype, int32_t device);
+
+/* Runs FoF on the particles (host-resident ones are first copied into
+ * plan-owned device memory on `stream`).  With out_location == CMH_DEVICE
+ * the catalog arrays stay in plan-owned device memory (valid until the next
+ * run or cmh_plan_destroy); with CMH_HOST they are copied to host arrays that
+ * cmh_catalog_free releases. */
+cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts,
+                        cmh_catalog *cat, int32_t want_member,
+                        int32_t out_location, void *stream);
+
+/* Changes the run parameters of a plan (same precision of positions). */
+cmh_status cmh_plan_set_params(cmh_plan *plan, const cmh_fof_params *params);
+
+void cmh_plan_destroy(cmh_plan *plan);
+
+/* ---- batched boxes: many independent domains in one launch sequence ----- */
+
+/* Runs `nbox` independent domains; box b uses params[b] and parts[b]
+ * (device-resident, same dtypes for all boxes).  The boxes' particles are
+ * processed together: one sort, one befriending pass and one reduction for
+ * the whole batch.  cats[b] receives box b's catalog (host arrays). */
+cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *parts,
+                             int32_t nbox, cmh_catalog *cats, void *stream);
+
+/* ---- run-parameter file (startup.c:109-314) ----------------------------- */
+
+/* The reference's tag/value run_parameters file.  Same tags, same rules:
+ * `%` starts a comment line, an unknown or repeated tag is an error, every
+ * tag must be present (startup.c:258-306).  `build_flags` selects the tags of
+ * optional builds: CMH_TAGS_VARLINK adds Omega and Origin_* (startup.c:240-256;
+ * Origin_* read as floating point here, the reference's INT typo is not
+ * kept), CMH_TAGS_INFOFILE adds InputInfoFile (LIGHTCONE + UNFORMATTED,
+ * startup.c:232-238). */
+#define CMH_TAGS_VARLINK 1
+#define CMH_TAGS_INFOFILE 2
+typedef struct cmh_run_parameters {
+  int32_t Nx, Ny, Nz, Px, Py, Pz;
+  double Lxmin, Lymin, Lzmin, Lxmax, Lymax, Lzmax;
+  int32_t Seed;
+  double Buffer, Boundarysize, Linklength, Nphalomin, SampInHalos, SampOutHalos;
+  int32_t InputStyle, Ninputfiles, Starting_file, Nread, Nwrite;
+  char InputFileBase[500];
+  char OutputFileBase[500];
+  double Omega, Origin_x, Origin_y, Origin_z;
+  char InputInfoFile[500];
+} cmh_run_parameters;
+
+cmh_status cmh_read_parameterfile(const char *fname, int32_t build_flags,
+                                  cmh_run_parameters *out);
+
+/* FoF parameters of one rank's domain from the run parameters, as
+ * Set_Params derives rmin/rmax (startup.c:33-47) for rank `task` of
+ * Nx*Ny*Nz. */
+cmh_status cmh_params_from_run(const cmh_run_parameters *rp, int32_t task,
+                               int32_t periodic, cmh_fof_params *out);
+
+/* ---- catalog writers (FOF.c:546-957) ------------------------------------ */
+
+#define CMH_OUT_UNFORMATTED 1u /* -DOUTPUT_UNFORMATTED */
+#define CMH_OUT_PARTICLES 2u   /* -DOUTPUT_PARTICLES   */
+#define CMH_OUT_PARTICLE_ID 4u /* -DPARTICLE_ID        */
+
+/* Writes "<base>.<task>" in the reference's layout (Output_Halos,
+ * FOF.c:546-913); no file when there are no halos, as there.  With
+ * CMH_OUT_PARTICLES the members of each halo follow its record, head first
+ * then in ascending processing order (the reference walks its ring from the
+ * head); `cat` must carry member, member_proc and member_pos (host) and
+ * `parts` (host) supplies velocities and, with CMH_OUT_PARTICLE_ID, IDs. */
+cmh_status cmh_write_halos(const char *base, int32_t task, const cmh_catalog *cat,
+                           const cmh_particles *parts, uint32_t flags);
+
+/* Writes "<base>.info" (Output_Info, FOF.c:917-957) for one task grid. */
+cmh_status cmh_write_info(const char *base, const cmh_run_parameters *rp,
+                          const int64_t *nhalos_per_task, int32_t ntask);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CMH_FOF_H */

@@ -99,6 +99,8 @@ SIGNATURES = {
     "cmh_plan_destroy": (None, [C.c_void_p]),
     "cmh_fof_run_batch": (C.c_int, [C.POINTER(FofParams), C.POINTER(Particles), C.c_int32,
                                     C.POINTER(Catalog), C.c_void_p]),
+    "cmh_fof_labels_noalloc": (C.c_int, [C.POINTER(FofParams), C.c_void_p, C.c_int32,
+                                         C.c_int64, C.c_void_p, C.c_void_p]),
     "cmh_read_parameterfile": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(RunParameters)]),
     "cmh_params_from_run": (C.c_int, [C.POINTER(RunParameters), C.c_int32, C.c_int32,
                                       C.POINTER(FofParams)]),

@@ -183,6 +183,28 @@ void cmh_plan_destroy(cmh_plan *plan);
 cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *parts,
                              int32_t nbox, cmh_catalog *cats, void *stream);
 
+/* ---- allocation-free labels for small sets ------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a framework already holds nearly all of it, allocation is banned
+ * after start-up, or a plugin host lends out only its own buffers): FoF group
+ * labels with no cudaMalloc/cudaFree and no allocating library call.  Its
+ * scratch is a fixed array in the library's device memory (about 1.5 MB on
+ * every GPU that loads the library, held until exit).
+ *   pos   : device array, n x 3 of pos_dtype, all inside [lo-b, hi+b]
+ *           (otherwise CMH_ERR_DOMAIN)
+ *   label : device array, n entries; label[i] = lowest index of i's group,
+ *           groups being the connected components of the reference's pair
+ *           predicate in double (FOF.c:351-357)
+ * Limits: n <= 65536 (CMH_ERR_CAPACITY beyond), non-periodic, constant
+ * linking length.  The first call on a device looks up the array's address
+ * with that device current; make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race.
+ * Returns after the stream has finished the work. */
+cmh_status cmh_fof_labels_noalloc(const cmh_fof_params *params, const void *pos,
+                                  int32_t pos_dtype, int64_t n, uint32_t *label,
+                                  void *stream);
+
 /* ---- run-parameter file (startup.c:109-314) ----------------------------- */
 
 /* The reference's tag/value run_parameters file.  Same tags, same rules:

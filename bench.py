@@ -249,6 +249,10 @@ def run_ours(args):
                    "n_halos": st["nhalos"], "n_groups": st["n_groups"],
                    "n_fine_cells": st["n_cells"], "cell_factor": st["cell_factor"],
                    "pair_tests": st["n_pair_tests"], "rechecks": st["n_rechecks"],
+                   "cell_pairs": st["n_cell_pairs"], "root_skips": st["n_root_skips"],
+                   "unions": st["n_unions"], "find_steps": st["n_find_steps"],
+                   "scan_iters": st["n_scan_iters"], "window_iters": st["n_window_iters"],
+                   "dense_tops": st["n_dense_tops"],
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "inputs (400 MB) larger than L2; no flush"},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},

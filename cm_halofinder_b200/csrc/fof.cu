@@ -319,95 +319,267 @@ __device__ __forceinline__ double box_dist2(const Geom &g, double x, double y, d
   return ex * ex + ey * ey + ez * ez;
 }
 
+// Per-thread tallies of the befriending kernel, flushed once per warp.
+struct BfStats {
+  unsigned long long tests = 0, rechecks = 0, cand = 0, skips = 0, unions = 0, steps = 0;
+  unsigned long long scan = 0, window = 0;
+};
+
 // Link fine cells a and b if any pair of their particles is linked.  The
 // cells are internally connected, so one linked pair joins them entirely.
+// `ra` caches a root of a's component: it may be stale (a root that was hooked
+// since), but it stays in a's component, so "b reaches ra" still proves that
+// a and b are already joined.
 template <class PT, bool FP32>
-__device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t b, int bx, int by,
-                                         int bz, uint32_t sa, uint32_t ea,
+__device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra, uint32_t b,
+                                         int bx, int by, int bz, uint32_t sa, uint32_t ea,
                                          const uint32_t *__restrict__ run_start,
                                          const SPos<PT> *__restrict__ spos, uint32_t *parent,
-                                         Counters *ctr, unsigned long long &tests,
-                                         unsigned long long &rechecks) {
-  if (uf_find(parent, a) == uf_find(parent, b)) return;
+                                         Counters *ctr, BfStats &st) {
+  st.cand++;
+  const uint32_t pb = __ldcg(parent + b);
+  st.steps++;
+  if (pb == ra) { st.skips++; return; }
+  const uint32_t rb = (pb == b) ? b : uf_find_n(parent, pb, st.steps);
+  if (rb == ra) { st.skips++; return; }
+  ra = uf_find_n(parent, ra, st.steps);
+  if (rb == ra) { st.skips++; return; }
   const uint32_t sb = __ldg(run_start + b), eb = __ldg(run_start + b + 1);
   for (uint32_t i = sa; i < ea; i++) {
     const SPos<PT> p = spos[i];
     // particles farther than the linking length from cell b's box cannot link
     if (box_dist2(g, (double)p.x, (double)p.y, (double)p.z, bx, by, bz) > g.prune_sq) continue;
     for (uint32_t j = sb; j < eb; j++) {
-      tests++;
-      if (linked<PT, FP32>(p, spos[j], g, rechecks)) {
-        uf_union(parent, a, b, ctr);
+      st.tests++;
+      if (linked<PT, FP32>(p, spos[j], g, st.rechecks)) {
+        uf_union(parent, ra, rb, ctr);
+        st.unions++;
+        ra = uf_find_n(parent, ra, st.steps);
         return;
       }
     }
   }
 }
 
-// One thread per occupied fine cell a.  Candidates are the fine cells b > a
-// (key order, so each unordered pair is visited once) within W fine cells
-// on every axis; they live in a's top cell (after a) and the 13 forward top
-// cells.  phase 0 visits cells within one fine cell, phase 1 the rest, so
-// that the dense cores are joined before the far pairs are tried.
+// Candidates of fine cell a are the fine cells b > a (key order, so each
+// unordered pair is visited once) within W fine cells on every axis; they
+// live in a's top cell (after a) and the 13 forward top cells.
+//
+// Fast path, one thread per fine cell: the 14 top-cell ranges are loaded at
+// once; when no range holds more than kSimple candidate cells (the common
+// case away from clumps), the first of each is loaded at once too and the
+// cell is finished in two L2 round trips.  Other cells are queued for the
+// warp path below.
+constexpr uint32_t kSimple = 2;
+
 template <class PT, bool FP32>
-__global__ void __launch_bounds__(kT) k_befriend(
+__global__ void __launch_bounds__(kT) k_befriend_simple(
     Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint32_t *__restrict__ nruns, const uint32_t *__restrict__ top_first,
-    const uint32_t *__restrict__ top_end, const uint32_t *__restrict__ top_slot,
-    const int32_t *__restrict__ maps, uint32_t dense_min, const SPos<PT> *__restrict__ spos,
-    uint32_t *parent, int phase, Counters *ctr) {
+    const uint32_t *__restrict__ top_end, const SPos<PT> *__restrict__ spos, uint32_t *parent,
+    uint32_t *__restrict__ queue, uint32_t *qcount, Counters *ctr) {
   const uint32_t R = *nruns;
   const int k = g.k, W = g.W;
-  unsigned long long tests = 0, rechecks = 0;
+  const int lane = threadIdx.x & 31;
+  BfStats st;
   for (int64_t ai = gtid(); ai < R; ai += gstride()) {
     const uint32_t a = (uint32_t)ai;
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const int tx = gx / k, ty = gy / k, tz = gz / k;
-    const uint32_t sa = run_start[a], ea = run_start[a + 1];
+    uint32_t R0[14], NN[14];
+#pragma unroll
     for (int nb = 0; nb < 14; nb++) {
       const int ux = tx + kFwd[nb][0], uy = ty + kFwd[nb][1], uz = tz + kFwd[nb][2];
-      if (ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]) continue;
-      const uint64_t tb = ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux;
-      const uint32_t f = top_first[tb], e = top_end[tb];
-      const uint32_t r0 = nb == 0 ? a + 1 : f;
-      if (r0 >= e) continue;
-      if (e - f <= dense_min) {
-        for (uint32_t r = r0; r < e; r++) {
-          const uint64_t qg = run_g[r];
-          const int bx = (int)(qg & kM21), by = (int)((qg >> 21) & kM21), bz = (int)(qg >> 42);
-          const int cheb = max(abs(bx - gx), max(abs(by - gy), abs(bz - gz)));
-          if (cheb > W || (phase == 0 && cheb > 1) || (phase == 1 && cheb <= 1)) continue;
-          try_link<PT, FP32>(g, a, r, bx, by, bz, sa, ea, run_start, spos, parent, ctr, tests,
-                             rechecks);
+      const bool in = !(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]);
+      const uint64_t tb = in ? ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux : 0;
+      const uint32_t f = in ? top_first[tb] : 0u, e = in ? top_end[tb] : 0u;
+      R0[nb] = nb == 0 ? a + 1 : f;
+      NN[nb] = e > R0[nb] ? e - R0[nb] : 0u;
+    }
+    bool simple = true;
+#pragma unroll
+    for (int nb = 0; nb < 14; nb++) simple &= NN[nb] <= kSimple;
+    const unsigned active = __activemask();
+    const unsigned qmask = __ballot_sync(active, !simple);
+    if (qmask) {
+      const int leader = __ffs(qmask) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(qcount, (uint32_t)__popc(qmask));
+      base = __shfl_sync(active, base, leader);
+      if (!simple) queue[base + __popc(qmask & ((1u << lane) - 1u))] = a;
+    }
+    if (!simple) continue;
+    uint64_t Q[14];
+#pragma unroll
+    for (int nb = 0; nb < 14; nb++) Q[nb] = NN[nb] ? run_g[R0[nb]] : 0ull;
+    uint32_t ra = 0xffffffffu, sa = 0, ea = 0;
+#pragma unroll
+    for (int nb = 0; nb < 14; nb++) {
+      for (uint32_t q = 0; q < NN[nb]; q++) {
+        const uint64_t qg = q == 0 ? Q[nb] : run_g[R0[nb] + q];
+        const int bx = (int)(qg & kM21), by = (int)((qg >> 21) & kM21), bz = (int)(qg >> 42);
+        st.scan++;
+        if (max(abs(bx - gx), max(abs(by - gy), abs(bz - gz))) > W) continue;
+        if (ra == 0xffffffffu) {
+          ra = __ldcg(parent + a);
+          sa = run_start[a];
+          ea = run_start[a + 1];
         }
-      } else {
-        const int32_t *map = maps + (uint64_t)top_slot[tb] * g.k3;
-        const int x0 = max(gx - W, ux * k), x1 = min(gx + W, ux * k + k - 1);
-        const int y0 = max(gy - W, uy * k), y1 = min(gy + W, uy * k + k - 1);
-        const int z0 = max(gz - W, uz * k), z1 = min(gz + W, uz * k + k - 1);
-        for (int cz = z0; cz <= z1; cz++)
-          for (int cy = y0; cy <= y1; cy++)
-            for (int cx = x0; cx <= x1; cx++) {
-              const int cheb = max(abs(cx - gx), max(abs(cy - gy), abs(cz - gz)));
-              if ((phase == 0 && cheb > 1) || (phase == 1 && cheb <= 1)) continue;
-              const int32_t r = map[((cz - uz * k) * k + (cy - uy * k)) * k + (cx - ux * k)];
-              if (r < 0 || (uint32_t)r < r0) continue;
-              try_link<PT, FP32>(g, a, (uint32_t)r, cx, cy, cz, sa, ea, run_start, spos, parent,
-                                 ctr, tests, rechecks);
-            }
+        try_link<PT, FP32>(g, a, ra, R0[nb] + q, bx, by, bz, sa, ea, run_start, spos, parent,
+                           ctr, st);
       }
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    st.tests += __shfl_down_sync(0xffffffffu, st.tests, d);
+    st.rechecks += __shfl_down_sync(0xffffffffu, st.rechecks, d);
+    st.cand += __shfl_down_sync(0xffffffffu, st.cand, d);
+    st.skips += __shfl_down_sync(0xffffffffu, st.skips, d);
+    st.unions += __shfl_down_sync(0xffffffffu, st.unions, d);
+    st.steps += __shfl_down_sync(0xffffffffu, st.steps, d);
+    st.scan += __shfl_down_sync(0xffffffffu, st.scan, d);
+  }
+  if (lane == 0) {
+    if (st.tests) atomicAdd(&ctr->pair_tests, st.tests);
+    if (st.rechecks) atomicAdd(&ctr->rechecks, st.rechecks);
+    if (st.cand) atomicAdd(&ctr->cand_pairs, st.cand);
+    if (st.skips) atomicAdd(&ctr->root_skips, st.skips);
+    if (st.unions) atomicAdd(&ctr->unions, st.unions);
+    if (st.steps) atomicAdd(&ctr->find_steps, st.steps);
+    if (st.scan) atomicAdd(&ctr->scan_iters, st.scan);
+  }
+}
+
+// Warp path, one warp per queued fine cell a.  Lanes 0..13 fetch the 14
+// top-cell ranges at once; the candidate slots of all 14 (fine cells of small
+// top cells, map slots of the window in dense ones) are then flattened and
+// taken 32 at a time, so a cell costs a few L2 round trips instead of one per
+// slot.
+template <class PT, bool FP32>
+__global__ void __launch_bounds__(kT) k_befriend(
+    Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
+    const uint32_t *__restrict__ queue, const uint32_t *__restrict__ qcount,
+    const uint32_t *__restrict__ top_first, const uint32_t *__restrict__ top_end,
+    const uint32_t *__restrict__ top_slot, const int32_t *__restrict__ maps, uint32_t dense_min,
+    const SPos<PT> *__restrict__ spos, uint32_t *parent, Counters *ctr) {
+  const uint32_t NQ = *qcount;
+  const int k = g.k, W = g.W;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = gstride() >> 5;
+  BfStats st;
+  for (int64_t qi = gtid() >> 5; qi < NQ; qi += nwarps) {
+    const uint32_t a = queue[qi];
+    const uint64_t pg = run_g[a];
+    const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
+    const int tx = gx / k, ty = gy / k, tz = gz / k;
+    const uint32_t sa = run_start[a], ea = run_start[a + 1];
+    uint32_t ra = __ldcg(parent + a);
+    // lane l < 14 describes neighbour top cell l
+    uint32_t r0 = 0, nsparse = 0, nslots = 0, mapbase = 0;
+    int x0 = 0, y0 = 0, z0 = 0, nx = 1, ny = 1, ox = 0, oy = 0, oz = 0;
+    if (lane < 14) {
+      const int ux = tx + kFwd[lane][0], uy = ty + kFwd[lane][1], uz = tz + kFwd[lane][2];
+      if (!(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2])) {
+        const uint64_t tb = ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux;
+        const uint32_t f = top_first[tb], e = top_end[tb];
+        r0 = lane == 0 ? a + 1 : f;
+        if (r0 < e) {
+          if (e - f <= dense_min) {
+            nsparse = e - r0;
+          } else {
+            x0 = max(gx - W, ux * k);
+            const int x1 = min(gx + W, ux * k + k - 1);
+            y0 = max(gy - W, uy * k);
+            const int y1 = min(gy + W, uy * k + k - 1);
+            // in a's own top cell only rows at or after a's hold cells b > a
+            z0 = max(lane == 0 ? gz : gz - W, uz * k);
+            const int z1 = min(gz + W, uz * k + k - 1);
+            if (x1 >= x0 && y1 >= y0 && z1 >= z0) {
+              nx = x1 - x0 + 1;
+              ny = y1 - y0 + 1;
+              nslots = (uint32_t)(nx * ny * (z1 - z0 + 1));
+              mapbase = top_slot[tb];
+              ox = ux * k;
+              oy = uy * k;
+              oz = uz * k;
+            }
+          }
+        }
+      }
+    }
+    const uint32_t cnt = nsparse + nslots;
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t excl = incl - cnt;
+    for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      // the neighbour top cell l whose items hold j
+      int l = 0;
+#pragma unroll
+      for (int q = 1; q < 14; q++)
+        if (j >= __shfl_sync(0xffffffffu, excl, q)) l = q;
+      const uint32_t l_excl = __shfl_sync(0xffffffffu, excl, l);
+      const uint32_t l_r0 = __shfl_sync(0xffffffffu, r0, l);
+      const uint32_t l_ns = __shfl_sync(0xffffffffu, nsparse, l);
+      const int l_x0 = __shfl_sync(0xffffffffu, x0, l), l_y0 = __shfl_sync(0xffffffffu, y0, l),
+                l_z0 = __shfl_sync(0xffffffffu, z0, l), l_nx = __shfl_sync(0xffffffffu, nx, l),
+                l_ny = __shfl_sync(0xffffffffu, ny, l), l_ox = __shfl_sync(0xffffffffu, ox, l),
+                l_oy = __shfl_sync(0xffffffffu, oy, l), l_oz = __shfl_sync(0xffffffffu, oz, l);
+      const uint32_t l_map = __shfl_sync(0xffffffffu, mapbase, l);
+      if (j >= total) continue;
+      const uint32_t off = j - l_excl;
+      uint32_t r;
+      int bx, by, bz;
+      if (off < l_ns) {
+        st.scan++;
+        r = l_r0 + off;
+        const uint64_t qg = run_g[r];
+        bx = (int)(qg & kM21);
+        by = (int)((qg >> 21) & kM21);
+        bz = (int)(qg >> 42);
+        if (max(abs(bx - gx), max(abs(by - gy), abs(bz - gz))) > W) continue;
+      } else {
+        st.window++;
+        const uint32_t sl = off - l_ns;
+        bx = l_x0 + (int)(sl % (uint32_t)l_nx);
+        by = l_y0 + (int)((sl / (uint32_t)l_nx) % (uint32_t)l_ny);
+        bz = l_z0 + (int)(sl / (uint32_t)(l_nx * l_ny));
+        const int32_t rr =
+            maps[(uint64_t)l_map * g.k3 + (uint64_t)(((bz - l_oz) * k + (by - l_oy)) * k + (bx - l_ox))];
+        if (rr < 0 || (uint32_t)rr < l_r0) continue;
+        r = (uint32_t)rr;
+      }
+      try_link<PT, FP32>(g, a, ra, r, bx, by, bz, sa, ea, run_start, spos, parent, ctr, st);
     }
   }
   // one atomic per warp for the counters
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) {
-    tests += __shfl_down_sync(0xffffffffu, tests, d);
-    rechecks += __shfl_down_sync(0xffffffffu, rechecks, d);
+    st.tests += __shfl_down_sync(0xffffffffu, st.tests, d);
+    st.rechecks += __shfl_down_sync(0xffffffffu, st.rechecks, d);
+    st.cand += __shfl_down_sync(0xffffffffu, st.cand, d);
+    st.skips += __shfl_down_sync(0xffffffffu, st.skips, d);
+    st.unions += __shfl_down_sync(0xffffffffu, st.unions, d);
+    st.steps += __shfl_down_sync(0xffffffffu, st.steps, d);
+    st.scan += __shfl_down_sync(0xffffffffu, st.scan, d);
+    st.window += __shfl_down_sync(0xffffffffu, st.window, d);
   }
   if ((threadIdx.x & 31) == 0) {
-    if (tests) atomicAdd(&ctr->pair_tests, tests);
-    if (rechecks) atomicAdd(&ctr->rechecks, rechecks);
+    if (st.tests) atomicAdd(&ctr->pair_tests, st.tests);
+    if (st.rechecks) atomicAdd(&ctr->rechecks, st.rechecks);
+    if (st.cand) atomicAdd(&ctr->cand_pairs, st.cand);
+    if (st.skips) atomicAdd(&ctr->root_skips, st.skips);
+    if (st.unions) atomicAdd(&ctr->unions, st.unions);
+    if (st.steps) atomicAdd(&ctr->find_steps, st.steps);
+    if (st.scan) atomicAdd(&ctr->scan_iters, st.scan);
+    if (st.window) atomicAdd(&ctr->window_iters, st.window);
   }
 }
 
@@ -892,23 +1064,28 @@ void Plan::run_typed(const cmh_particles &parts, bool want_member, cudaStream_t 
   k_iota<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);
   CMH_LAUNCHED();
   CMH_CUDA(cudaEventRecord(stage_ev[2], s));
-  for (int phase = 0; phase < 2; phase++) {
-    if (fp32)
-      k_befriend<PT, true><<<gr, kT, 0, s>>>(g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(),
-                                             sc + 2, b_top_first.as<uint32_t>(),
-                                             b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),
-                                             b_maps.as<int32_t>(), dense_min,
-                                             b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(),
-                                             phase, c);
-    else
-      k_befriend<PT, false><<<gr, kT, 0, s>>>(g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(),
-                                              sc + 2, b_top_first.as<uint32_t>(),
-                                              b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),
-                                              b_maps.as<int32_t>(), dense_min,
-                                              b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(),
-                                              phase, c);
-    CMH_LAUNCHED();
+  // fast path for every cell, queue of the crowded ones, warp path for those
+  uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
+  CMH_CUDA(cudaMemsetAsync(sc + 6, 0, sizeof(uint32_t), s));
+  const unsigned gw = grid_for(RR * 32, kT);  // one warp per queued cell
+#define CMH_BEFRIEND(FP)                                                                      \
+  k_befriend_simple<PT, FP><<<gr, kT, 0, s>>>(g, b_run_start.as<uint32_t>(),                 \
+                                              b_run_g.as<uint64_t>(), sc + 2,                 \
+                                              b_top_first.as<uint32_t>(),                     \
+                                              b_top_end.as<uint32_t>(), b_spos.as<SPos<PT>>(), \
+                                              b_parent.as<uint32_t>(), queue, sc + 6, c);     \
+  CMH_LAUNCHED();                                                                             \
+  k_befriend<PT, FP><<<gw, kT, 0, s>>>(                                                       \
+      g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(), queue, sc + 6,                  \
+      b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),       \
+      b_maps.as<int32_t>(), dense_min, b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);  \
+  CMH_LAUNCHED()
+  if (fp32) {
+    CMH_BEFRIEND(true);
+  } else {
+    CMH_BEFRIEND(false);
   }
+#undef CMH_BEFRIEND
   k_compress<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);
   CMH_LAUNCHED();
   CMH_CUDA(cudaEventRecord(stage_ev[3], s));
@@ -1053,6 +1230,13 @@ void Plan::run_typed(const cmh_particles &parts, bool want_member, cudaStream_t 
   stats.n_edge_warn = (int64_t)hc.nwarn;
   stats.n_pair_tests = (int64_t)hc.c.pair_tests;
   stats.n_rechecks = (int64_t)hc.c.rechecks;
+  stats.n_cell_pairs = (int64_t)hc.c.cand_pairs;
+  stats.n_root_skips = (int64_t)hc.c.root_skips;
+  stats.n_unions = (int64_t)hc.c.unions;
+  stats.n_find_steps = (int64_t)hc.c.find_steps;
+  stats.n_scan_iters = (int64_t)hc.c.scan_iters;
+  stats.n_window_iters = (int64_t)hc.c.window_iters;
+  stats.n_dense_tops = (int64_t)nd;
   stats.n_member_conflicts = (int64_t)hc.c.member_conflicts;
   stats.cell_factor = g.k;
   stats.key_bits = key_bits;

@@ -55,6 +55,12 @@ struct Counters {
   unsigned long long member_conflicts;
   unsigned int uf_giveups;     // union loops that hit their iteration cap
   unsigned int domain_errors;  // particles outside [rmin, rmax] after ingest
+  unsigned long long cand_pairs;   // fine-cell pairs within reach
+  unsigned long long root_skips;   // ... already in one component
+  unsigned long long unions;       // ... joined by a linked particle pair
+  unsigned long long find_steps;   // parent loads in the befriending finds
+  unsigned long long scan_iters;   // fine cells scanned in sparse top cells
+  unsigned long long window_iters; // map slots visited in dense top cells
 };
 
 // FP32 band around l^2: returns the thresholds t_lo < fl32(l2) < t_hi such
@@ -98,6 +104,21 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
     uint32_t gp = __ldcg(parent + p);
     if (gp == p) return p;
     __stcg(parent + x, gp);  // path halving: gp is an ancestor of x
+    x = gp;
+  }
+}
+
+// find() that also counts its parent loads
+__device__ __forceinline__ uint32_t uf_find_n(uint32_t *parent, uint32_t x,
+                                              unsigned long long &steps) {
+  while (true) {
+    uint32_t p = __ldcg(parent + x);
+    steps++;
+    if (p == x) return x;
+    uint32_t gp = __ldcg(parent + p);
+    steps++;
+    if (gp == p) return p;
+    __stcg(parent + x, gp);
     x = gp;
   }
 }

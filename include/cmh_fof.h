@@ -106,6 +106,13 @@ typedef struct cmh_stats {
   float stage_ms[8];       /* ingest, sort, cells, befriend, groups, sums,
                               catalog, members (CUDA events on the stream)    */
   int32_t n_launches;      /* kernels launched by the run                     */
+  int64_t n_cell_pairs;    /* fine-cell pairs within linking reach            */
+  int64_t n_root_skips;    /* ... found already joined                        */
+  int64_t n_unions;        /* ... joined by a linked particle pair            */
+  int64_t n_find_steps;    /* union-find parent loads while befriending       */
+  int64_t n_scan_iters;    /* fine cells scanned in sparse top cells          */
+  int64_t n_window_iters;  /* map slots visited in dense top cells            */
+  int64_t n_dense_tops;    /* top cells with a fine-cell map                  */
 } cmh_stats;
 
 /* Halo catalog in the layout of the reference's unformatted records

@@ -71,7 +71,7 @@ Plan::~Plan() {
                    &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
                    &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
                    &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
-                   &in_pos, &in_vel};
+                   &in_pos, &in_vel, &b_dense_range};
   for (DevBuf *b : all) b->release();
   if (h_scal) cudaFreeHost(h_scal);
   if (ev0) cudaEventDestroy(ev0);

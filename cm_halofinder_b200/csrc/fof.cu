@@ -115,7 +115,7 @@ __device__ __forceinline__ void emit_one(const Geom &g, uint32_t p, const double
                                          SPos<PT> *ppos) {
   int gi[3];
 #pragma unroll
-  for (int a = 0; a < 3; a++) gi[a] = fine_index(c[a], g.rmin[a], g.h, g.G[a]);
+  for (int a = 0; a < 3; a++) gi[a] = fine_index(c[a], g.rmin[a], g.inv_h, g.G[a]);
   const int k = g.k;
   const uint64_t top = ((uint64_t)(gi[2] / k) * g.T[1] + (gi[1] / k)) * g.T[0] + (gi[0] / k);
   const uint64_t sub = ((uint64_t)(gi[2] % k) * k + (gi[1] % k)) * k + (gi[0] % k);
@@ -135,14 +135,14 @@ template <class PT>
 __global__ void __launch_bounds__(kT) k_ingest_emit(
     const PT *__restrict__ pos, int64_t n, Geom g, const uint32_t *__restrict__ keep,
     const uint32_t *__restrict__ keep_scan, const uint32_t *__restrict__ img_scan,
-    const uint32_t *__restrict__ nkept_ptr, uint64_t *__restrict__ keys,
-    uint32_t *__restrict__ vals, SPos<PT> *__restrict__ ppos) {
+    const uint32_t *__restrict__ nimg, const uint32_t *__restrict__ nkept_ptr,
+    uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, SPos<PT> *__restrict__ ppos) {
   const uint32_t nkept = *nkept_ptr;
   for (int64_t i = gtid(); i < n; i += gstride()) {
     if (!keep[i]) continue;
     double x[3] = {as_d(pos[3 * i]), as_d(pos[3 * i + 1]), as_d(pos[3 * i + 2])};
     emit_one<PT>(g, keep_scan[i], x, (uint32_t)i, keys, vals, ppos);
-    if (!g.periodic) continue;
+    if (!g.periodic || nimg[i] == 0) continue;
     uint32_t q = nkept + img_scan[i];
     double cm[3], cp[3];
     bool okm[3], okp[3];
@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ 
                                                    const uint32_t *__restrict__ dscan,
                                                    uint32_t dense_min,
                                                    uint32_t *__restrict__ top_slot,
+                                                   uint2 *__restrict__ dense_range,
                                                    int32_t *__restrict__ maps) {
   const uint32_t R = *nruns;
   const int k = g.k;
@@ -257,7 +258,10 @@ __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ 
     const uint32_t f = top_first[t];
     if (top_end[t] - f <= dense_min) continue;
     const uint32_t slot = dscan[f];  // the first run of the cell carries the slot
-    if (dflag[r]) top_slot[t] = slot;
+    if (dflag[r]) {
+      top_slot[t] = slot;
+      dense_range[slot] = make_uint2(f, top_end[t]);
+    }
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const uint64_t sub = ((uint64_t)(gz % k) * k + (gy % k)) * k + (gx % k);
     maps[(uint64_t)slot * g.k3 + sub] = (int32_t)r;
@@ -325,6 +329,31 @@ struct BfStats {
   unsigned long long scan = 0, window = 0;
 };
 
+// Whether any particle of fine cell a (particles [sa, ea)) is linked to any
+// particle of fine cell b (fine coordinates bx, by, bz).  Particles of a
+// farther than the linking length from b's box are skipped.  Every 16
+// particles of a, `apart()` is asked whether a and b are still in different
+// components (another thread may have joined them meanwhile); if not, the
+// search stops and reports no link, which is then harmless.
+template <class PT, bool FP32, class Apart>
+__device__ __forceinline__ bool cells_linked(const Geom &g, uint32_t b, int bx, int by, int bz,
+                                             uint32_t sa, uint32_t ea,
+                                             const uint32_t *__restrict__ run_start,
+                                             const SPos<PT> *__restrict__ spos, BfStats &st,
+                                             Apart apart) {
+  const uint32_t sb = __ldg(run_start + b), eb = __ldg(run_start + b + 1);
+  for (uint32_t i = sa; i < ea; i++) {
+    if (((i - sa) & 15) == 15 && !apart()) return false;
+    const SPos<PT> p = spos[i];
+    if (box_dist2(g, (double)p.x, (double)p.y, (double)p.z, bx, by, bz) > g.prune_sq) continue;
+    for (uint32_t j = sb; j < eb; j++) {
+      st.tests++;
+      if (linked<PT, FP32>(p, spos[j], g, st.rechecks)) return true;
+    }
+  }
+  return false;
+}
+
 // Link fine cells a and b if any pair of their particles is linked.  The
 // cells are internally connected, so one linked pair joins them entirely.
 // `ra` caches a root of a's component: it may be stale (a root that was hooked
@@ -344,21 +373,132 @@ __device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra
   if (rb == ra) { st.skips++; return; }
   ra = uf_find_n(parent, ra, st.steps);
   if (rb == ra) { st.skips++; return; }
-  const uint32_t sb = __ldg(run_start + b), eb = __ldg(run_start + b + 1);
-  for (uint32_t i = sa; i < ea; i++) {
-    const SPos<PT> p = spos[i];
-    // particles farther than the linking length from cell b's box cannot link
-    if (box_dist2(g, (double)p.x, (double)p.y, (double)p.z, bx, by, bz) > g.prune_sq) continue;
-    for (uint32_t j = sb; j < eb; j++) {
-      st.tests++;
-      if (linked<PT, FP32>(p, spos[j], g, st.rechecks)) {
-        uf_union(parent, ra, rb, ctr);
-        st.unions++;
-        ra = uf_find_n(parent, ra, st.steps);
-        return;
-      }
-    }
+  auto apart = [&]() {
+    return uf_find_n(parent, a, st.steps) != uf_find_n(parent, b, st.steps);
+  };
+  if (cells_linked<PT, FP32>(g, b, bx, by, bz, sa, ea, run_start, spos, st, apart)) {
+    uf_union(parent, ra, rb, ctr);
+    st.unions++;
+    ra = uf_find_n(parent, ra, st.steps);
   }
+}
+
+// Union-find in shared memory over the fine cells of one top cell (local
+// indices), same hook-to-min rule as the global one.
+__device__ __forceinline__ uint32_t lfind(volatile uint32_t *lp, uint32_t x) {
+  while (true) {
+    const uint32_t p = lp[x];
+    if (p == x) return x;
+    const uint32_t gp = lp[p];
+    if (gp == p) return p;
+    lp[x] = gp;
+    x = gp;
+  }
+}
+
+__device__ __forceinline__ void lunion(uint32_t *lp, uint32_t a, uint32_t b, Counters *ctr) {
+  for (int it = 0; it < kUnionCap; it++) {
+    a = lfind(lp, a);
+    b = lfind(lp, b);
+    if (a == b) return;
+    if (a < b) {
+      const uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    const uint32_t old = atomicCAS(lp + a, a, b);
+    if (old == a) return;
+    a = old;
+  }
+  atomicAdd(&ctr->uf_giveups, 1u);
+}
+
+// Dense top cells, one CTA each: the fine-cell pairs inside the top cell are
+// joined with a shared-memory union-find (neighbours found through the top
+// cell's fine-cell map), near pairs before far ones; then every fine cell's
+// global parent is set to its local root.  Links that cross the top cell's
+// faces are left to the global passes.
+template <class PT, bool FP32>
+__global__ void __launch_bounds__(128) k_befriend_dense(
+    Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
+    const uint2 *__restrict__ dense_range, const uint32_t *__restrict__ ndense, uint32_t *next,
+    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos, uint32_t *parent,
+    Counters *ctr) {
+  extern __shared__ uint32_t lpar[];
+  __shared__ uint32_t s_slot;
+  const uint32_t nd = *ndense;
+  const int k = g.k, W = g.W;
+  BfStats st;
+  while (true) {
+    // top cells are taken from an atomic counter: their sizes differ widely
+    if (threadIdx.x == 0) s_slot = atomicAdd(next, 1u);
+    __syncthreads();
+    const uint32_t slot = s_slot;
+    __syncthreads();
+    if (slot >= nd) break;
+    const uint2 fr = dense_range[slot];
+    const uint32_t f = fr.x, n = fr.y - fr.x;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) lpar[i] = i;
+    __syncthreads();
+    const int32_t *map = maps + (uint64_t)slot * g.k3;
+    for (int pass = 0; pass < 2; pass++) {
+      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t a = f + i;
+        const uint64_t pg = run_g[a];
+        const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
+        const int sx = gx % k, sy = gy % k, sz = gz % k;
+        const uint32_t sa = run_start[a], ea = run_start[a + 1];
+        for (int dz = 0; dz <= W; dz++)
+          for (int dy = -W; dy <= W; dy++)
+            for (int dx = -W; dx <= W; dx++) {
+              if (dz == 0 && (dy < 0 || (dy == 0 && dx <= 0))) continue;  // forward only
+              const int cheb = max(abs(dx), max(abs(dy), dz));
+              if ((pass == 0) != (cheb <= 1)) continue;
+              const int tx = sx + dx, ty = sy + dy, tz = sz + dz;
+              if (tx < 0 || ty < 0 || tx >= k || ty >= k || tz >= k) continue;
+              const int32_t r = map[(tz * k + ty) * k + tx];
+              if (r < 0) continue;
+              st.cand++;
+              const uint32_t lj = (uint32_t)r - f;
+              const uint32_t ri = lfind(lpar, i), rj = lfind(lpar, lj);
+              if (ri == rj) {
+                st.skips++;
+                continue;
+              }
+              auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
+              if (cells_linked<PT, FP32>(g, (uint32_t)r, gx + dx, gy + dy, gz + dz, sa, ea,
+                                         run_start, spos, st, apart)) {
+                lunion(lpar, ri, rj, ctr);
+                st.unions++;
+              }
+            }
+      }
+      __syncthreads();
+    }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) parent[f + i] = f + lfind(lpar, i);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    st.tests += __shfl_down_sync(0xffffffffu, st.tests, d);
+    st.rechecks += __shfl_down_sync(0xffffffffu, st.rechecks, d);
+    st.cand += __shfl_down_sync(0xffffffffu, st.cand, d);
+    st.skips += __shfl_down_sync(0xffffffffu, st.skips, d);
+    st.unions += __shfl_down_sync(0xffffffffu, st.unions, d);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (st.tests) atomicAdd(&ctr->pair_tests, st.tests);
+    if (st.rechecks) atomicAdd(&ctr->rechecks, st.rechecks);
+    if (st.cand) atomicAdd(&ctr->cand_pairs, st.cand);
+    if (st.skips) atomicAdd(&ctr->root_skips, st.skips);
+    if (st.unions) atomicAdd(&ctr->unions, st.unions);
+  }
+}
+
+// Whether fine cell a's neighbour top cell in direction (ox, oy, oz) lies
+// within W fine cells of a (s = a's fine coordinates inside its top cell).
+__device__ __forceinline__ bool reaches(int s, int o, int k, int W) {
+  return o == 0 || (o > 0 ? s >= k - W : s <= W - 1);
 }
 
 // Candidates of fine cell a are the fine cells b > a (key order, so each
@@ -373,11 +513,12 @@ __device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra
 constexpr uint32_t kSimple = 2;
 
 template <class PT, bool FP32>
-__global__ void __launch_bounds__(kT) k_befriend_simple(
+__global__ void __launch_bounds__(kT, 5) k_befriend_simple(
     Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint32_t *__restrict__ nruns, const uint32_t *__restrict__ top_first,
-    const uint32_t *__restrict__ top_end, const SPos<PT> *__restrict__ spos, uint32_t *parent,
-    uint32_t *__restrict__ queue, uint32_t *qcount, Counters *ctr) {
+    const uint32_t *__restrict__ top_end, uint32_t dense_min,
+    const SPos<PT> *__restrict__ spos, uint32_t *parent, uint32_t *__restrict__ queue,
+    uint32_t *qcount, Counters *ctr) {
   const uint32_t R = *nruns;
   const int k = g.k, W = g.W;
   const int lane = threadIdx.x & 31;
@@ -387,15 +528,21 @@ __global__ void __launch_bounds__(kT) k_befriend_simple(
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const int tx = gx / k, ty = gy / k, tz = gz / k;
+    const int sx = gx - tx * k, sy = gy - ty * k, sz = gz - tz * k;
     uint32_t R0[14], NN[14];
 #pragma unroll
     for (int nb = 0; nb < 14; nb++) {
       const int ux = tx + kFwd[nb][0], uy = ty + kFwd[nb][1], uz = tz + kFwd[nb][2];
-      const bool in = !(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]);
+      // a top cell more than W fine cells away from a is skipped without a load
+      const bool in = !(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]) &&
+                      reaches(sx, kFwd[nb][0], k, W) && reaches(sy, kFwd[nb][1], k, W) &&
+                      reaches(sz, kFwd[nb][2], k, W);
       const uint64_t tb = in ? ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux : 0;
       const uint32_t f = in ? top_first[tb] : 0u, e = in ? top_end[tb] : 0u;
       R0[nb] = nb == 0 ? a + 1 : f;
       NN[nb] = e > R0[nb] ? e - R0[nb] : 0u;
+      // pairs inside a dense top cell are joined by k_befriend_dense
+      if (nb == 0 && e - f > dense_min) NN[nb] = 0u;
     }
     bool simple = true;
 #pragma unroll
@@ -456,35 +603,47 @@ __global__ void __launch_bounds__(kT) k_befriend_simple(
 // top-cell ranges at once; the candidate slots of all 14 (fine cells of small
 // top cells, map slots of the window in dense ones) are then flattened and
 // taken 32 at a time, so a cell costs a few L2 round trips instead of one per
-// slot.
-template <class PT, bool FP32>
+// slot.  Warps take cells from `next` (an atomic counter) as they finish, so
+// a few expensive cells do not hold back a whole static share.  PHASE 0
+// visits the candidates within one fine cell, PHASE 1 the farther ones, so
+// that a dense neighbourhood is joined (and compressed) before its far pairs
+// are tried and most of those become root skips.
+template <class PT, bool FP32, int PHASE>
 __global__ void __launch_bounds__(kT) k_befriend(
     Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
-    const uint32_t *__restrict__ queue, const uint32_t *__restrict__ qcount,
+    const uint32_t *__restrict__ queue, const uint32_t *__restrict__ qcount, uint32_t *next,
     const uint32_t *__restrict__ top_first, const uint32_t *__restrict__ top_end,
     const uint32_t *__restrict__ top_slot, const int32_t *__restrict__ maps, uint32_t dense_min,
     const SPos<PT> *__restrict__ spos, uint32_t *parent, Counters *ctr) {
   const uint32_t NQ = *qcount;
   const int k = g.k, W = g.W;
   const int lane = threadIdx.x & 31;
-  const int64_t nwarps = gstride() >> 5;
   BfStats st;
-  for (int64_t qi = gtid() >> 5; qi < NQ; qi += nwarps) {
+  while (true) {
+    uint32_t qi = 0;
+    if (lane == 0) qi = atomicAdd(next, 1u);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= NQ) break;
     const uint32_t a = queue[qi];
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const int tx = gx / k, ty = gy / k, tz = gz / k;
     const uint32_t sa = run_start[a], ea = run_start[a + 1];
     uint32_t ra = __ldcg(parent + a);
+    const int sx = gx - tx * k, sy = gy - ty * k, sz = gz - tz * k;
     // lane l < 14 describes neighbour top cell l
     uint32_t r0 = 0, nsparse = 0, nslots = 0, mapbase = 0;
     int x0 = 0, y0 = 0, z0 = 0, nx = 1, ny = 1, ox = 0, oy = 0, oz = 0;
     if (lane < 14) {
       const int ux = tx + kFwd[lane][0], uy = ty + kFwd[lane][1], uz = tz + kFwd[lane][2];
-      if (!(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2])) {
+      if (!(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]) &&
+          reaches(sx, kFwd[lane][0], k, W) && reaches(sy, kFwd[lane][1], k, W) &&
+          reaches(sz, kFwd[lane][2], k, W)) {
         const uint64_t tb = ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux;
         const uint32_t f = top_first[tb], e = top_end[tb];
         r0 = lane == 0 ? a + 1 : f;
+        // pairs inside a dense top cell are joined by k_befriend_dense
+        if (lane == 0 && e - f > dense_min) r0 = e;
         if (r0 < e) {
           if (e - f <= dense_min) {
             nsparse = e - r0;
@@ -556,6 +715,8 @@ __global__ void __launch_bounds__(kT) k_befriend(
         if (rr < 0 || (uint32_t)rr < l_r0) continue;
         r = (uint32_t)rr;
       }
+      const int cheb = max(abs(bx - gx), max(abs(by - gy), abs(bz - gz)));
+      if ((PHASE == 0 && cheb > 1) || (PHASE == 1 && cheb <= 1)) continue;
       try_link<PT, FP32>(g, a, ra, r, bx, by, bz, sa, ea, run_start, spos, parent, ctr, st);
     }
   }
@@ -915,6 +1076,7 @@ void Plan::setup_geometry(int64_t n_in) {
   band_thresholds(g.linksq, pos_dtype == CMH_FLOAT64 ? 8 : 4, &g.t_lo, &g.t_hi);
   // fine cell: any two points of a cell are closer than minlink
   g.h = minlink * (1.0 - 0x1p-20) / std::sqrt(3.0);
+  g.inv_h = 1.0 / g.h;
   g.W = (int)std::floor(maxlink / g.h * (1.0 + 1e-6)) + 1;
   double vol = 1.0;
   for (int a = 0; a < 3; a++) {
@@ -1002,7 +1164,7 @@ void Plan::run_typed(const cmh_particles &parts, bool want_member, cudaStream_t 
   if (n > 0) {
     k_ingest_emit<PT><<<grid_for(n, kT), kT, 0, s>>>(
         pos, n, g, b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(), b_img_scan.as<uint32_t>(),
-        sc + 0, b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
+        b_nimg.as<uint32_t>(), sc + 0, b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
     CMH_LAUNCHED();
   }
   CMH_CUDA(cudaEventRecord(stage_ev[0], s));
@@ -1051,12 +1213,13 @@ void Plan::run_typed(const cmh_particles &parts, bool want_member, cudaStream_t 
   CMH_CUDA(cudaStreamSynchronize(s));
   const int64_t nd = h_scal[3];
   b_maps.ensure(std::max<int64_t>(nd, 1) * g.k3 * 4);
+  b_dense_range.ensure(std::max<int64_t>(nd, 1) * sizeof(uint2));
   if (nd > 0) {
     CMH_CUDA(cudaMemsetAsync(b_maps.p, 0xff, nd * g.k3 * 4, s));
     k_dense_maps<<<gr, kT, 0, s>>>(b_run_g.as<uint64_t>(), g, sc + 2, b_top_first.as<uint32_t>(),
                                    b_top_end.as<uint32_t>(), b_rtmp1.as<uint32_t>(),
                                    b_rtmp2.as<uint32_t>(), dense_min, b_top_slot.as<uint32_t>(),
-                                   b_maps.as<int32_t>());
+                                   b_dense_range.as<uint2>(), b_maps.as<int32_t>());
     CMH_LAUNCHED();
   }
   // ---- befriending ----
@@ -1064,19 +1227,41 @@ void Plan::run_typed(const cmh_particles &parts, bool want_member, cudaStream_t 
   k_iota<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);
   CMH_LAUNCHED();
   CMH_CUDA(cudaEventRecord(stage_ev[2], s));
-  // fast path for every cell, queue of the crowded ones, warp path for those
+  // dense top cells joined inside (CTA each), then a fast path for every
+  // cell, a queue of the crowded ones and a warp path for those
   uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
-  CMH_CUDA(cudaMemsetAsync(sc + 6, 0, sizeof(uint32_t), s));
+  // sc[6] queue length, sc[7..9] work counters of the dense and warp passes
+  CMH_CUDA(cudaMemsetAsync(sc + 6, 0, 4 * sizeof(uint32_t), s));
   const unsigned gw = grid_for(RR * 32, kT);  // one warp per queued cell
+  const size_t dsm = (size_t)g.k3 * sizeof(uint32_t);
+  const unsigned gd = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nd, (int64_t)kSMs * 16));
 #define CMH_BEFRIEND(FP)                                                                      \
+  if (nd > 0) {                                                                               \
+    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<PT, FP>,                                   \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));    \
+    k_befriend_dense<PT, FP><<<gd, 128, dsm, s>>>(g, b_run_start.as<uint32_t>(),              \
+                                                  b_run_g.as<uint64_t>(),                     \
+                                                  b_dense_range.as<uint2>(), sc + 3, sc + 7,  \
+                                                  b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), \
+                                                  b_parent.as<uint32_t>(), c);                \
+    CMH_LAUNCHED();                                                                           \
+  }                                                                                           \
   k_befriend_simple<PT, FP><<<gr, kT, 0, s>>>(g, b_run_start.as<uint32_t>(),                 \
                                               b_run_g.as<uint64_t>(), sc + 2,                 \
                                               b_top_first.as<uint32_t>(),                     \
-                                              b_top_end.as<uint32_t>(), b_spos.as<SPos<PT>>(), \
-                                              b_parent.as<uint32_t>(), queue, sc + 6, c);     \
+                                              b_top_end.as<uint32_t>(), dense_min,            \
+                                              b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), \
+                                              queue, sc + 6, c);                              \
   CMH_LAUNCHED();                                                                             \
-  k_befriend<PT, FP><<<gw, kT, 0, s>>>(                                                       \
-      g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(), queue, sc + 6,                  \
+  k_befriend<PT, FP, 0><<<gw, kT, 0, s>>>(                                                    \
+      g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(), queue, sc + 6, sc + 8,          \
+      b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),       \
+      b_maps.as<int32_t>(), dense_min, b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);  \
+  CMH_LAUNCHED();                                                                             \
+  k_compress<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);                              \
+  CMH_LAUNCHED();                                                                             \
+  k_befriend<PT, FP, 1><<<gw, kT, 0, s>>>(                                                    \
+      g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(), queue, sc + 6, sc + 9,          \
       b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),       \
       b_maps.as<int32_t>(), dense_min, b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);  \
   CMH_LAUNCHED()

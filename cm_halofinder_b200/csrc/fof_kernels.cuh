@@ -28,6 +28,7 @@ struct Geom {
   double maxlink;        // largest linking length (edge warning, pruning)
   double prune_sq;       // (maxlink * (1 + 1e-5))^2: pairs of cells farther apart never link
   double h;              // fine cell side, <= minimum linking length / sqrt(3)
+  double inv_h;          // 1 / h
   double nphalomin;
   float t_lo, t_hi;      // FP32 band: d2 < t_lo links, d2 > t_hi does not
   int periodic;
@@ -82,9 +83,11 @@ __host__ __device__ inline void band_thresholds(double l2, int ulps, float *t_lo
   *t_hi = fhi;
 }
 
-// Fine-cell index along one axis: floor((x - rmin) / h), in double.
-__device__ __forceinline__ int fine_index(double x, double rmin, double h, int G) {
-  double q = __ddiv_rn(__dsub_rn(x, rmin), h);
+// Fine-cell index along one axis: floor((x - rmin) * (1/h)), in double.  Two
+// points with the same index are within h (1 + 4e-16 * index) of each other
+// along the axis, far inside the 2^-20 margin that sizes h.
+__device__ __forceinline__ int fine_index(double x, double rmin, double inv_h, int G) {
+  double q = __dmul_rn(__dsub_rn(x, rmin), inv_h);
   int g = (int)floor(q);
   g = g < 0 ? 0 : g;
   return g >= G ? G - 1 : g;

@@ -39,6 +39,7 @@ struct Plan : public cmh_plan {
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
   DevBuf in_pos, in_vel;  // device copies of host-resident particles
+  DevBuf b_dense_range;   // first/end fine cell of each dense top cell
 
   Plan(const cmh_fof_params &p, int pos_dtype, int device);
   ~Plan() override;

@@ -65,18 +65,25 @@ __global__ void __launch_bounds__(kThreads) k_rs_hist(const K *__restrict__ keys
   hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// The scatter pass ranks a 4096-key tile with 512 threads x 8 keys: fewer
+// registers per thread than the counting pass's layout, so more warps hide
+// the memory latency.
+constexpr int kSThreads = 512;
+constexpr int kSWarps = kSThreads / 32;
+constexpr int kSIPT = kTile / kSThreads;  // 8
+
 template <class K>
 struct ScatterSmem {
   K keys[kTile];
   uint32_t vals[kTile];
-  uint32_t wcnt[kWarps][kBins];
+  uint32_t wcnt[kSWarps][kBins];
   uint32_t dstart[kBins];
   uint32_t gofs[kBins];
-  uint32_t warp_sums[kWarps];
+  uint32_t warp_sums[kSWarps];
 };
 
 template <class K>
-__global__ void __launch_bounds__(kThreads) k_rs_scatter(
+__global__ void __launch_bounds__(kSThreads) k_rs_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
     K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n, int shift,
     const uint32_t *__restrict__ hist_scan, int64_t ntiles) {
@@ -85,21 +92,20 @@ __global__ void __launch_bounds__(kThreads) k_rs_scatter(
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t base = (int64_t)blockIdx.x * kTile;
 
-  for (int i = threadIdx.x; i < kWarps * kBins; i += kThreads) (&sm.wcnt[0][0])[i] = 0;
-  sm.gofs[threadIdx.x] = hist_scan[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+  for (int i = threadIdx.x; i < kSWarps * kBins; i += kSThreads) (&sm.wcnt[0][0])[i] = 0;
+  if (threadIdx.x < kBins) sm.gofs[threadIdx.x] = hist_scan[(int64_t)threadIdx.x * ntiles + blockIdx.x];
   __syncthreads();
 
   const uint32_t lt_mask = (1u << lane) - 1u;
-  K k[kIPT];
-  uint32_t v[kIPT], rank[kIPT], dg[kIPT];
+  K k[kSIPT];
+  uint32_t v[kSIPT], rank[kSIPT];
 #pragma unroll
-  for (int j = 0; j < kIPT; j++) {
-    const int64_t i = base + (int64_t)warp * 32 * kIPT + j * 32 + lane;
+  for (int j = 0; j < kSIPT; j++) {
+    const int64_t i = base + (int64_t)warp * 32 * kSIPT + j * 32 + lane;
     const bool valid = i < n;
     k[j] = valid ? keys_in[i] : K(0);
     v[j] = valid ? vals_in[i] : 0u;
     const uint32_t d = valid ? digit_of(k[j], shift) : (uint32_t)kBins;
-    dg[j] = d;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t lt = peers & lt_mask;
     uint32_t c = 0;
@@ -111,30 +117,43 @@ __global__ void __launch_bounds__(kThreads) k_rs_scatter(
   }
   __syncthreads();
   {
+    // per digit: exclusive prefix over the warps, then over the digits
     const int d = threadIdx.x;
     uint32_t acc = 0;
+    if (d < kBins) {
 #pragma unroll
-    for (int w = 0; w < kWarps; w++) {
-      uint32_t t = sm.wcnt[w][d];
-      sm.wcnt[w][d] = acc;
-      acc += t;
+      for (int w = 0; w < kSWarps; w++) {
+        uint32_t t = sm.wcnt[w][d];
+        sm.wcnt[w][d] = acc;
+        acc += t;
+      }
     }
-    sm.dstart[d] = block_exclusive(acc, sm.warp_sums);
+    uint32_t inc = warp_inclusive(acc);
+    if (lane == 31) sm.warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = lane < kSWarps ? sm.warp_sums[lane] : 0;
+      uint32_t wi = warp_inclusive(w);
+      if (lane < kSWarps) sm.warp_sums[lane] = wi - w;
+    }
+    __syncthreads();
+    if (d < kBins) sm.dstart[d] = inc - acc + sm.warp_sums[warp];
   }
   __syncthreads();
+  const int64_t rem = n - base;
 #pragma unroll
-  for (int j = 0; j < kIPT; j++) {
-    const uint32_t d = dg[j];
-    if (d < (uint32_t)kBins) {
+  for (int j = 0; j < kSIPT; j++) {
+    const int64_t i = base + (int64_t)warp * 32 * kSIPT + j * 32 + lane;
+    if (i < n) {
+      const uint32_t d = digit_of(k[j], shift);
       const uint32_t lp = sm.dstart[d] + sm.wcnt[warp][d] + rank[j];
       sm.keys[lp] = k[j];
       sm.vals[lp] = v[j];
     }
   }
   __syncthreads();
-  const int64_t rem = n - base;
   const int tile_n = rem < kTile ? (int)rem : kTile;
-  for (int q = threadIdx.x; q < tile_n; q += kThreads) {
+  for (int q = threadIdx.x; q < tile_n; q += kSThreads) {
     const K key = sm.keys[q];
     const uint32_t d = digit_of(key, shift);
     const uint32_t g = sm.gofs[d] + (uint32_t)q - sm.dstart[d];
@@ -165,7 +184,7 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
     k_rs_hist<K><<<(unsigned)ntiles, kThreads, 0, s>>>(src_k, n, shift, hist, ntiles);
     CMH_LAUNCHED();
     exclusive_scan_u32(hist, hist_scan, hn, nullptr, scan_tmp, s);
-    k_rs_scatter<K><<<(unsigned)ntiles, kThreads, smem, s>>>(src_k, src_v, dst_k, dst_v, n,
+    k_rs_scatter<K><<<(unsigned)ntiles, kSThreads, smem, s>>>(src_k, src_v, dst_k, dst_v, n,
                                                               shift, hist_scan, ntiles);
     CMH_LAUNCHED();
     std::swap(src_k, dst_k);

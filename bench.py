@@ -172,21 +172,33 @@ def run_ours(args):
             ms = float(t.item())
         return ms, st, stages, launches
 
+    def stage_breakdown(plan):
+        # one eager (non-graph) step: the library records CUDA events between
+        # its stages on this stream
+        plan.set_graph(False)
+        cat = plan.run(pos, vel, out="device", stream=stream)
+        plan.set_graph(not args.no_graph)
+        return cat.stats.as_dict()["stage_ms"]
+
     cfg_fast = FofConfig.from_workload(w, precision=args.precision)
     plan = Plan(cfg_fast, pos_dtype=w.pos.dtype, device=local)
+    plan.set_graph(not args.no_graph)
     clocks = ClockSampler(local)
     for _ in range(args.warmup):
         plan.run(pos, vel, out="device", stream=stream)
     clocks.start()
-    ms, st, stages, launches = timed(plan, args.steps, 0)
+    ms, st, _, launches = timed(plan, args.steps, 0)
     clk = clocks.stop()
+    stages = stage_breakdown(plan)
     value = n * world / (ms * 1e-3) / 1e6
 
     plain = None
     if not args.no_plain and args.precision != "fp64":
         plan_p = Plan(FofConfig.from_workload(w, precision="fp64"), pos_dtype=w.pos.dtype,
                       device=local)
-        ms_p, st_p, stages_p, _ = timed(plan_p, max(1, args.steps), args.warmup)
+        plan_p.set_graph(not args.no_graph)
+        ms_p, st_p, _, _ = timed(plan_p, max(1, args.steps), args.warmup)
+        stages_p = stage_breakdown(plan_p)
         plain = {"value": n * world / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
                  "n_pair_tests": st_p["n_pair_tests"],
                  "stage_ms": {k: round(v, 4) for k, v in stages_p.items()},
@@ -256,6 +268,7 @@ def run_ours(args):
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "inputs (400 MB) larger than L2; no flush"},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "stage_ms_note": "per-stage CUDA-event times of one eager step after the timed graph replays",
         "plain_fp64": plain,
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -368,6 +381,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="issue every step eagerly")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-timeout", type=float, default=20.0)
     ap.add_argument("--traffic", type=float, default=None,

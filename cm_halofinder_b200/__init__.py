@@ -218,6 +218,36 @@ class Plan:
         finally:
             self._L.cmh_catalog_free(C.byref(cat))
 
+    def set_graph(self, enable: bool):
+        """Replay runs of a repeated shape from a captured CUDA graph."""
+        _abi.check(self._L.cmh_plan_set_graph(self._h, int(bool(enable))))
+
+    def run_batch(self, configs, positions, velocities, stream=None):
+        """Many independent boxes in one run (one sort, one befriending pass,
+        one reduction for all of them); positions/velocities are torch CUDA
+        tensors.  Returns one host Catalog per box."""
+        nb = len(configs)
+        P = (_abi.FofParams * nb)(*[c.to_c() for c in configs])
+        keep = [P]
+        parts = (_abi.Particles * nb)()
+        for b in range(nb):
+            pos, vel = positions[b], velocities[b]
+            parts[b] = _abi.Particles(n=int(pos.shape[0]), pos_dtype=self._tdt(pos),
+                                      vel_dtype=self._tdt(vel), pos=self._ptr(pos),
+                                      vel=self._ptr(vel), id=None, location=CMH_DEVICE)
+        cats = (_abi.Catalog * nb)()
+        sp = 0 if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream")
+                                        else int(stream))
+        _abi.check(self._L.cmh_plan_run_batch(self._h, P, parts, nb, cats, C.c_void_p(sp)))
+        del keep
+        out = []
+        for b in range(nb):
+            try:
+                out.append(_host_catalog(cats[b]))
+            finally:
+                self._L.cmh_catalog_free(C.byref(cats[b]))
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.cmh_plan_destroy(self._h)

@@ -99,6 +99,9 @@ SIGNATURES = {
                                C.c_int32, C.c_void_p]),
     "cmh_plan_set_params": (C.c_int, [C.c_void_p, C.POINTER(FofParams)]),
     "cmh_plan_destroy": (None, [C.c_void_p]),
+    "cmh_plan_set_graph": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cmh_plan_run_batch": (C.c_int, [C.c_void_p, C.POINTER(FofParams), C.POINTER(Particles),
+                                     C.c_int32, C.POINTER(Catalog), C.c_void_p]),
     "cmh_fof_run_batch": (C.c_int, [C.POINTER(FofParams), C.POINTER(Particles), C.c_int32,
                                     C.POINTER(Catalog), C.c_void_p]),
     "cmh_fof_labels_noalloc": (C.c_int, [C.POINTER(FofParams), C.c_void_p, C.c_int32,

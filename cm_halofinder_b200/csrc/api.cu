@@ -55,7 +55,6 @@ Plan::Plan(const cmh_fof_params &p, int pdt, int dev) : device(dev), pos_dtype(p
   int major = 0;
   CMH_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
   if (major < 10) fail(CMH_ERR_NO_DEVICE, "the FoF kernels are built for sm_100a (B200)");
-  CMH_CUDA(cudaMallocHost(&h_scal, 64 * sizeof(uint32_t)));
   CMH_CUDA(cudaEventCreate(&ev0));
   CMH_CUDA(cudaEventCreate(&ev1));
   for (cudaEvent_t &e : stage_ev) CMH_CUDA(cudaEventCreate(&e));
@@ -64,16 +63,17 @@ Plan::Plan(const cmh_fof_params &p, int pdt, int dev) : device(dev), pos_dtype(p
 
 Plan::~Plan() {
   cudaSetDevice(device);
-  DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_keep, &b_nimg,
-                   &b_keep_scan, &b_img_scan, &b_keys, &b_keys_alt, &b_vals, &b_vals_alt,
-                   &b_ppos, &b_spos, &b_run_of, &b_run_start, &b_run_g, &b_top_first,
-                   &b_top_end, &b_top_slot, &b_rtmp1, &b_rtmp2, &b_maps, &b_parent, &b_count,
-                   &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
-                   &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
-                   &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
-                   &in_pos, &in_vel, &b_dense_range};
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (cap_stream) cudaStreamDestroy(cap_stream);
+  DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd, &b_keep,
+                   &b_nimg, &b_keep_scan, &b_img_scan, &b_keys, &b_keys_alt, &b_vals,
+                   &b_vals_alt, &b_ppos, &b_spos, &b_run_of, &b_run_start, &b_run_g,
+                   &b_run_box, &b_top_first, &b_top_end, &b_top_slot, &b_rtmp1, &b_rtmp2,
+                   &b_maps, &b_dense_range, &b_parent, &b_count, &b_head, &b_cand_of_root,
+                   &b_cand_root, &b_sums, &b_warn, &b_own, &b_own_scan, &b_okeys, &b_ovals,
+                   &b_okeys_alt, &b_ovals_alt, &b_props, &b_head_out, &b_cat_of_cand,
+                   &b_member, &b_member_proc, &b_member_pos, &in_pos, &in_vel};
   for (DevBuf *b : all) b->release();
-  if (h_scal) cudaFreeHost(h_scal);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   for (cudaEvent_t e : stage_ev)
@@ -132,11 +132,15 @@ void check_parts(const cmh_particles *parts) {
     cmh::fail(CMH_ERR_CAPACITY, "more than 2^32 particles in one domain");
 }
 
-// Copies the plan's last catalog to host arrays owned by `cat`.
-void catalog_to_host(Plan &pl, cmh_catalog *cat, bool want_member, int64_t n_in,
-                     cudaStream_t s) {
-  const int64_t nh = pl.out_nhalos;
-  const int hs = pl.geom.hs;
+// Copies box b's part of the plan's last catalog to host arrays owned by
+// `cat` (a run's catalog lists the boxes one after another).
+void catalog_to_host(Plan &pl, cmh_catalog *cat, bool want_member, int b, cudaStream_t s) {
+  const int nbox = (int)pl.boxes_host.size();
+  const int64_t nh = pl.boxd_host[5 * nbox + b];
+  const int64_t h0 = pl.boxd_host[6 * nbox + b];
+  const int64_t n_in = pl.boxes_host[b].n;
+  const int64_t i0 = (int64_t)pl.boxes_host[b].in_base;
+  const int hs = pl.hs;
   cat->nhalos = nh;
   cat->halosize = hs;
   cat->location = CMH_HOST;
@@ -156,26 +160,36 @@ void catalog_to_host(Plan &pl, cmh_catalog *cat, bool want_member, int64_t n_in,
       (want_member && (!cat->member || !cat->member_proc || !cat->member_pos)))
     cmh::fail(CMH_ERR_OUT_OF_MEMORY, "host catalog allocation failed");
   if (nh > 0) {
-    CMH_CUDA(cudaMemcpyAsync(cat->props, pl.b_props.p, sizeof(float) * nh * hs,
-                             cudaMemcpyDeviceToHost, s));
-    CMH_CUDA(cudaMemcpyAsync(cat->head, pl.b_head_out.p, sizeof(uint32_t) * nh,
-                             cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->props, pl.b_props.as<float>() + h0 * hs,
+                             sizeof(float) * nh * hs, cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->head, pl.b_head_out.as<uint32_t>() + h0,
+                             sizeof(uint32_t) * nh, cudaMemcpyDeviceToHost, s));
   }
   if (want_member && n_in > 0) {
-    CMH_CUDA(cudaMemcpyAsync(cat->member, pl.b_member.p, sizeof(int64_t) * n_in,
-                             cudaMemcpyDeviceToHost, s));
-    CMH_CUDA(cudaMemcpyAsync(cat->member_proc, pl.b_member_proc.p, sizeof(uint32_t) * n_in,
-                             cudaMemcpyDeviceToHost, s));
-    CMH_CUDA(cudaMemcpyAsync(cat->member_pos, pl.b_member_pos.p, sizeof(float) * 3 * n_in,
-                             cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->member, pl.b_member.as<int64_t>() + i0,
+                             sizeof(int64_t) * n_in, cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->member_proc, pl.b_member_proc.as<uint32_t>() + i0,
+                             sizeof(uint32_t) * n_in, cudaMemcpyDeviceToHost, s));
+    CMH_CUDA(cudaMemcpyAsync(cat->member_pos, pl.b_member_pos.as<float>() + 3 * i0,
+                             sizeof(float) * 3 * n_in, cudaMemcpyDeviceToHost, s));
   }
   CMH_CUDA(cudaStreamSynchronize(s));
+  if (want_member && h0 > 0)
+    for (int64_t i = 0; i < n_in; i++)
+      if (cat->member[i] >= 0) cat->member[i] -= h0;
   cat->stats = pl.stats;
+  if (nbox > 1) {
+    cat->stats.n_in = n_in;
+    cat->stats.nhalos = nh;
+    cat->stats.n_images = pl.boxd_host[3 * nbox + b];
+    cat->stats.n_proc = (int64_t)pl.boxd_host[2 * nbox + b] + pl.boxd_host[3 * nbox + b];
+    cat->stats.n_out = n_in - pl.boxd_host[2 * nbox + b];
+  }
 }
 
 void catalog_on_device(Plan &pl, cmh_catalog *cat, bool want_member) {
   cat->nhalos = pl.out_nhalos;
-  cat->halosize = pl.geom.hs;
+  cat->halosize = pl.hs;
   cat->location = CMH_DEVICE;
   cat->props = pl.b_props.as<float>();
   cat->head = pl.b_head_out.as<uint32_t>();
@@ -249,7 +263,7 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog 
   }
   pl.run(dp, want_member != 0, s);
   if (out_location == CMH_DEVICE) catalog_on_device(pl, cat, want_member != 0);
-  else catalog_to_host(pl, cat, want_member != 0, parts->n, s);
+  else catalog_to_host(pl, cat, want_member != 0, 0, s);
   CMH_API_END
 }
 
@@ -300,7 +314,7 @@ cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
   }
   try {
     pl->run(dp, want_member != 0, s);
-    catalog_to_host(*pl, cat, want_member != 0, parts->n, s);
+    catalog_to_host(*pl, cat, want_member != 0, 0, s);
   } catch (...) {
     dpos.release();
     dvel.release();
@@ -310,6 +324,37 @@ cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
   dvel.release();
   CMH_API_END
 }
+
+namespace {
+void run_batch_on(Plan &pl, const cmh_fof_params *params, const cmh_particles *parts,
+                  int32_t nbox, cmh_catalog *cats, cudaStream_t s) {
+  std::vector<cmh::BoxSpec> specs(nbox);
+  for (int b = 0; b < nbox; b++) {
+    check_parts(&parts[b]);
+    if (parts[b].location != CMH_DEVICE)
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "batched runs take device-resident particles");
+    if (parts[b].pos_dtype != pl.pos_dtype)
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "all boxes of a batch share the position dtype");
+    if (params[b].precision != params[0].precision)
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "all boxes of a batch share the precision mode");
+    cmh::BoxSpec &sp = specs[b];
+    sp.params = params[b];
+    if (params[b].varlink) {
+      if (params[b].ltab_n < 2 || !params[b].ltab)
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "variable linking length needs a table");
+      sp.ltab.assign(params[b].ltab, params[b].ltab + params[b].ltab_n);
+    }
+    sp.params.ltab = nullptr;
+    sp.pos = parts[b].pos;
+    sp.vel = parts[b].vel;
+    sp.vel_f64 = parts[b].vel_dtype == CMH_FLOAT64;
+    sp.n = parts[b].n;
+  }
+  pl.fp32 = params[0].precision == CMH_FP32_RECHECK;
+  pl.run_batch(specs, false, s);
+  for (int b = 0; b < nbox; b++) catalog_to_host(pl, &cats[b], false, b, s);
+}
+}  // namespace
 
 cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *parts,
                              int32_t nbox, cmh_catalog *cats, void *stream) {
@@ -321,16 +366,27 @@ cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *
   int dev = 0;
   CMH_CUDA(cudaGetDevice(&dev));
   std::unique_ptr<Plan> pl(new Plan(params[0], parts[0].pos_dtype, dev));
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  for (int b = 0; b < nbox; b++) {
-    check_parts(&parts[b]);
-    if (parts[b].location != CMH_DEVICE)
-      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "batched runs take device-resident particles");
-    pl->set_params(params[b]);
-    pl->pos_dtype = parts[b].pos_dtype;
-    pl->run(parts[b], false, s);
-    catalog_to_host(*pl, &cats[b], false, parts[b].n, s);
-  }
+  pl->use_graph = false;
+  run_batch_on(*pl, params, parts, nbox, cats, static_cast<cudaStream_t>(stream));
+  CMH_API_END
+}
+
+cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,
+                              const cmh_particles *parts, int32_t nbox, cmh_catalog *cats,
+                              void *stream) {
+  CMH_API_BEGIN
+  if (!plan || !params || !parts || !cats || nbox < 1)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan, params, particles and catalogs are required");
+  for (int b = 0; b < nbox; b++) memset(&cats[b], 0, sizeof cats[b]);
+  run_batch_on(*static_cast<Plan *>(plan), params, parts, nbox, cats,
+               static_cast<cudaStream_t>(stream));
+  CMH_API_END
+}
+
+cmh_status cmh_plan_set_graph(cmh_plan *plan, int32_t enable) {
+  CMH_API_BEGIN
+  if (!plan) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan is required");
+  static_cast<Plan *>(plan)->use_graph = enable != 0;
   CMH_API_END
 }
 

@@ -61,12 +61,14 @@ void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n,
 // Stable LSD radix sort of (key u64, value u32) pairs on the low `bits` key
 // bits.  Result lands in keys/vals (the alt buffers are scratch); `tmp`
 // holds the digit count tables and `scan_tmp` the scratch of their scan.
+// `n` sizes the launches; with `n_dev` set, the element count is read from
+// device memory (at most n), so the sort needs no host synchronisation.
 void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
-                        uint32_t *vals_alt, int64_t n, int bits, DevBuf &tmp,
-                        DevBuf &scan_tmp, cudaStream_t s);
+                        uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
+                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s);
 // Same for 32-bit keys.
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
-                        uint32_t *vals_alt, int64_t n, int bits, DevBuf &tmp,
-                        DevBuf &scan_tmp, cudaStream_t s);
+                        uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
+                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s);
 
 }  // namespace cmh

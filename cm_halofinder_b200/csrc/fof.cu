@@ -1,6 +1,10 @@
 // The FoF hot path on one B200: ingest + periodic images, cell keys, radix
 // sort, fine-cell runs, befriending with a lock-free union-find, and the
-// segmented reductions that produce the halo catalog.
+// segmented reductions that produce the halo catalog.  A run holds one or
+// many independent domains ("boxes"); all of them go through the same
+// launches (one sort, one befriending pass, one reduction for the batch), and
+// no size is read back by the host until the run is issued, so a run can be
+// captured in a CUDA graph and replayed.
 //
 // Reference: src_v2/FOF.c (FOF, Befriend, Checkhalo, Output_Halos property
 // sums) and src_v2/read_data.c:409-424,785-816 (domain filter, ghost wrap).
@@ -10,9 +14,10 @@
 // the linking length whatever their position inside it, so every occupied
 // fine cell is one connected piece and union-find runs over cells, not
 // particles.  Fine cells are grouped k^3 to a top cell; the sort key is
-// (top cell, fine cell inside it), so a top cell's fine cells are contiguous
-// and the befriending step visits the 27-cell top stencil (self + 13
-// forward neighbours), exactly the cell loop of FOF.c:96-161 one level up.
+// (top cell, fine cell inside it), each box's top cells numbered after the
+// previous box's, so a top cell's fine cells are contiguous and the
+// befriending step visits the 27-cell top stencil (self + 13 forward
+// neighbours), exactly the cell loop of FOF.c:96-161 one level up.
 //
 // Pair predicate.  A pair of particles is linked iff the reference's double
 // expression ((dx*dx + dy*dy) + dz*dz) <= Linklength^2 holds (FOF.c:351-357),
@@ -33,6 +38,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "cmh_internal.cuh"
@@ -60,11 +66,27 @@ __device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * block
 
 template <class T> __device__ __forceinline__ double as_d(T v) { return (double)v; }
 
+// Index of the last entry of base[0..nb) that is <= x (base[0] == 0).
+__device__ __forceinline__ int box_search(const uint64_t *base, int nb, uint64_t x) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Copies the boxes' first input index (or first top cell) into shared memory.
+__device__ __forceinline__ void load_bases(const BoxDev *boxes, int nbox, uint64_t *s, bool tops) {
+  for (int b = threadIdx.x; b < nbox; b += blockDim.x) s[b] = tops ? boxes[b].top_base : boxes[b].in_base;
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Ingest: domain filter (read_data.c:409-424) and periodic images.
 // ---------------------------------------------------------------------------
 
-template <class PT>
 __device__ __forceinline__ bool in_domain(const Geom &g, const double x[3]) {
   bool ok = true;
 #pragma unroll
@@ -88,12 +110,25 @@ __device__ __forceinline__ bool image_coord(const Geom &g, double x, int a, int 
 }
 
 template <class PT>
-__global__ void __launch_bounds__(kT) k_ingest_count(const PT *__restrict__ pos, int64_t n,
-                                                     Geom g, uint32_t *__restrict__ keep,
+__device__ __forceinline__ void load_pos(const BoxDev &bx, uint64_t li, double x[3]) {
+  const PT *pos = static_cast<const PT *>(bx.pos);
+  x[0] = as_d(pos[3 * li]);
+  x[1] = as_d(pos[3 * li + 1]);
+  x[2] = as_d(pos[3 * li + 2]);
+}
+
+template <class PT>
+__global__ void __launch_bounds__(kT) k_ingest_count(const BoxDev *__restrict__ boxes, int nbox,
+                                                     int64_t n, uint32_t *__restrict__ keep,
                                                      uint32_t *__restrict__ nimg) {
+  __shared__ uint64_t s_base[kMaxBoxes];
+  load_bases(boxes, nbox, s_base, false);
   for (int64_t i = gtid(); i < n; i += gstride()) {
-    double x[3] = {as_d(pos[3 * i]), as_d(pos[3 * i + 1]), as_d(pos[3 * i + 2])};
-    const bool ok = in_domain<PT>(g, x);
+    const BoxDev &bx = boxes[box_search(s_base, nbox, (uint64_t)i)];
+    const Geom &g = bx.g;
+    double x[3];
+    load_pos<PT>(bx, (uint64_t)i - bx.in_base, x);
+    const bool ok = in_domain(g, x);
     uint32_t cnt = 0;
     if (ok && g.periodic) {
       int opt[3];
@@ -109,17 +144,47 @@ __global__ void __launch_bounds__(kT) k_ingest_count(const PT *__restrict__ pos,
   }
 }
 
+// Per box: kept and image counts, and the first processing index of the box
+// (its kept particles, then its images).  Sets the run's processed count,
+// clamped to the capacity `np_cap`.
+__global__ void k_box_totals(const BoxDev *__restrict__ boxes, int nbox, int64_t n,
+                             const uint32_t *__restrict__ keep_scan,
+                             const uint32_t *__restrict__ img_scan, DevScal *sc,
+                             uint32_t *__restrict__ boxd, uint32_t np_cap) {
+  // boxd layout: [kept_before | img_before | nkept | nimg | proc_base | halo_count | halo_base]
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint64_t acc = 0;
+  for (int b = 0; b < nbox; b++) {
+    const uint64_t i0 = boxes[b].in_base, i1 = i0 + boxes[b].n;
+    const uint32_t k0 = i0 < (uint64_t)n ? keep_scan[i0] : sc->kept_total;
+    const uint32_t k1 = i1 < (uint64_t)n ? keep_scan[i1] : sc->kept_total;
+    const uint32_t m0 = i0 < (uint64_t)n ? img_scan[i0] : sc->img_total;
+    const uint32_t m1 = i1 < (uint64_t)n ? img_scan[i1] : sc->img_total;
+    boxd[0 * nbox + b] = k0;
+    boxd[1 * nbox + b] = m0;
+    boxd[2 * nbox + b] = k1 - k0;
+    boxd[3 * nbox + b] = m1 - m0;
+    boxd[4 * nbox + b] = (uint32_t)acc;
+    acc += (uint64_t)(k1 - k0) + (m1 - m0);
+  }
+  const uint64_t np = acc;
+  sc->np_raw = np > 0xffffffffull ? 0xffffffffu : (uint32_t)np;
+  sc->np = np > np_cap ? np_cap : (uint32_t)np;
+  if (np > np_cap) atomicOr(&sc->overflow, 1u);
+}
+
 template <class PT>
-__device__ __forceinline__ void emit_one(const Geom &g, uint32_t p, const double c[3],
-                                         uint32_t src, uint64_t *keys, uint32_t *vals,
-                                         SPos<PT> *ppos) {
+__device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint64_t k3all,
+                                         uint32_t p, const double c[3], uint32_t src,
+                                         uint64_t *keys, uint32_t *vals, SPos<PT> *ppos) {
   int gi[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) gi[a] = fine_index(c[a], g.rmin[a], g.inv_h, g.G[a]);
   const int k = g.k;
-  const uint64_t top = ((uint64_t)(gi[2] / k) * g.T[1] + (gi[1] / k)) * g.T[0] + (gi[0] / k);
-  const uint64_t sub = ((uint64_t)(gi[2] % k) * k + (gi[1] % k)) * k + (gi[0] % k);
-  keys[p] = top * g.k3 + sub;
+  const int t[3] = {gi[0] / k, gi[1] / k, gi[2] / k};
+  const uint64_t top = top_base + ((uint64_t)t[2] * g.T[1] + t[1]) * g.T[0] + t[0];
+  const uint64_t sub = ((uint64_t)(gi[2] - t[2] * k) * k + (gi[1] - t[1] * k)) * k + (gi[0] - t[0] * k);
+  keys[p] = top * k3all + sub;
   vals[p] = p;
   SPos<PT> s;
   s.x = (PT)c[0];
@@ -129,21 +194,31 @@ __device__ __forceinline__ void emit_one(const Geom &g, uint32_t p, const double
   ppos[p] = s;
 }
 
-// Processing order: kept originals in input order, then the images grouped
-// by source particle and shift code (sz+1)*9 + (sy+1)*3 + (sx+1) ascending.
+// Processing order of a box: kept originals in input order, then the images
+// grouped by source particle and shift code (sz+1)*9 + (sy+1)*3 + (sx+1)
+// ascending.  Writes beyond the capacity are dropped (the run is then
+// repeated with more room).
 template <class PT>
 __global__ void __launch_bounds__(kT) k_ingest_emit(
-    const PT *__restrict__ pos, int64_t n, Geom g, const uint32_t *__restrict__ keep,
-    const uint32_t *__restrict__ keep_scan, const uint32_t *__restrict__ img_scan,
-    const uint32_t *__restrict__ nimg, const uint32_t *__restrict__ nkept_ptr,
-    uint64_t *__restrict__ keys, uint32_t *__restrict__ vals, SPos<PT> *__restrict__ ppos) {
-  const uint32_t nkept = *nkept_ptr;
+    const BoxDev *__restrict__ boxes, int nbox, int64_t n, uint64_t k3all,
+    const uint32_t *__restrict__ keep, const uint32_t *__restrict__ keep_scan,
+    const uint32_t *__restrict__ img_scan, const uint32_t *__restrict__ nimg,
+    const uint32_t *__restrict__ boxd, uint32_t np_cap, uint64_t *__restrict__ keys,
+    uint32_t *__restrict__ vals, SPos<PT> *__restrict__ ppos) {
+  __shared__ uint64_t s_base[kMaxBoxes];
+  load_bases(boxes, nbox, s_base, false);
   for (int64_t i = gtid(); i < n; i += gstride()) {
     if (!keep[i]) continue;
-    double x[3] = {as_d(pos[3 * i]), as_d(pos[3 * i + 1]), as_d(pos[3 * i + 2])};
-    emit_one<PT>(g, keep_scan[i], x, (uint32_t)i, keys, vals, ppos);
+    const int b = box_search(s_base, nbox, (uint64_t)i);
+    const BoxDev &bx = boxes[b];
+    const Geom &g = bx.g;
+    double x[3];
+    load_pos<PT>(bx, (uint64_t)i - bx.in_base, x);
+    const uint32_t pbase = boxd[4 * nbox + b];
+    const uint32_t p = pbase + (keep_scan[i] - boxd[0 * nbox + b]);
+    if (p < np_cap) emit_one<PT>(g, bx.top_base, k3all, p, x, (uint32_t)i, keys, vals, ppos);
     if (!g.periodic || nimg[i] == 0) continue;
-    uint32_t q = nkept + img_scan[i];
+    uint32_t q = pbase + boxd[2 * nbox + b] + (img_scan[i] - boxd[1 * nbox + b]);
     double cm[3], cp[3];
     bool okm[3], okp[3];
 #pragma unroll
@@ -163,7 +238,8 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
         else c[a] = x[a];
       }
       if (!ok) continue;
-      emit_one<PT>(g, q++, c, (uint32_t)i, keys, vals, ppos);
+      if (q < np_cap) emit_one<PT>(g, bx.top_base, k3all, q, c, (uint32_t)i, keys, vals, ppos);
+      q++;
     }
   }
 }
@@ -172,105 +248,145 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
 // Runs of equal fine-cell keys.
 // ---------------------------------------------------------------------------
 
+// Cell-ordered positions and run-start flags; flags are 0 past the processed
+// count so that the scan over the capacity counts only real runs.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_gather_flags(const uint64_t *__restrict__ keys,
                                                      const uint32_t *__restrict__ perm,
                                                      const SPos<PT> *__restrict__ ppos,
                                                      SPos<PT> *__restrict__ spos,
-                                                     uint32_t *__restrict__ flag, int64_t np) {
-  for (int64_t i = gtid(); i < np; i += gstride()) {
-    spos[i] = ppos[perm[i]];
-    flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+                                                     uint32_t *__restrict__ flag,
+                                                     const DevScal *__restrict__ sc,
+                                                     int64_t cap) {
+  const int64_t np = sc->np;
+  for (int64_t i = gtid(); i < cap; i += gstride()) {
+    if (i < np) {
+      spos[i] = ppos[perm[i]];
+      flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+    } else {
+      flag[i] = 0u;
+    }
   }
 }
 
 __global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ keys,
                                              const uint32_t *__restrict__ flag,
-                                             const uint32_t *__restrict__ run_scan, int64_t np,
-                                             Geom g, uint32_t *__restrict__ run_of,
+                                             const uint32_t *__restrict__ run_scan,
+                                             const BoxDev *__restrict__ boxes, int nbox,
+                                             uint64_t k3all, DevScal *sc,
+                                             uint32_t *__restrict__ run_of,
                                              uint32_t *__restrict__ run_start,
                                              uint64_t *__restrict__ run_g,
-                                             const uint32_t *__restrict__ nruns) {
-  const uint32_t R = *nruns;
+                                             uint16_t *__restrict__ run_box) {
+  __shared__ uint64_t s_base[kMaxBoxes];
+  load_bases(boxes, nbox, s_base, true);
+  const int64_t np = sc->np;
+  const uint32_t R = sc->R;
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const uint32_t rid = run_scan[i] + flag[i] - 1u;
     run_of[i] = rid;
     if (flag[i]) {
       run_start[rid] = (uint32_t)i;
       const uint64_t key = keys[i];
-      const uint64_t top = key / g.k3, sub = key % g.k3;
+      const uint64_t gtop = key / k3all, sub = key % k3all;
+      const int b = box_search(s_base, nbox, gtop);
+      const Geom &g = boxes[b].g;
+      const uint64_t top = gtop - s_base[b];
       const int k = g.k;
       const uint64_t tx = top % g.T[0], ty = (top / g.T[0]) % g.T[1], tz = top / ((uint64_t)g.T[0] * g.T[1]);
       const uint64_t sx = sub % k, sy = (sub / k) % k, sz = sub / ((uint64_t)k * k);
       const uint64_t gx = tx * k + sx, gy = ty * k + sy, gz = tz * k + sz;
       run_g[rid] = gx | (gy << 21) | (gz << 42);
+      run_box[rid] = (uint16_t)b;
     }
     if (i == np - 1) run_start[R] = (uint32_t)np;
   }
 }
 
-__device__ __forceinline__ uint64_t top_of_run(const Geom &g, uint64_t pg) {
+__device__ __forceinline__ uint64_t top_of_run(const BoxDev &bx, uint64_t pg) {
+  const Geom &g = bx.g;
   const int k = g.k;
   const uint64_t gx = pg & kM21, gy = (pg >> 21) & kM21, gz = pg >> 42;
-  return ((gz / k) * g.T[1] + gy / k) * g.T[0] + gx / k;
+  return bx.top_base + ((gz / k) * g.T[1] + gy / k) * g.T[0] + gx / k;
 }
 
-__global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ run_g, Geom g,
-                                                   const uint32_t *__restrict__ nruns,
+__global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ run_g,
+                                                   const uint16_t *__restrict__ run_box,
+                                                   const BoxDev *__restrict__ boxes,
+                                                   const DevScal *__restrict__ sc,
                                                    uint32_t *__restrict__ top_first,
                                                    uint32_t *__restrict__ top_end) {
-  const uint32_t R = *nruns;
+  const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
-    const uint64_t t = top_of_run(g, run_g[r]);
-    if (r == 0 || top_of_run(g, run_g[r - 1]) != t) top_first[t] = (uint32_t)r;
-    if (r == R - 1 || top_of_run(g, run_g[r + 1]) != t) top_end[t] = (uint32_t)(r + 1);
+    const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
+    if (r == 0 || top_of_run(boxes[run_box[r - 1]], run_g[r - 1]) != t) top_first[t] = (uint32_t)r;
+    if (r == R - 1 || top_of_run(boxes[run_box[r + 1]], run_g[r + 1]) != t)
+      top_end[t] = (uint32_t)(r + 1);
   }
 }
 
-__global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__ run_g, Geom g,
-                                                    const uint32_t *__restrict__ nruns,
+// 1 on the first fine cell of a top cell with more than dense_min fine cells
+// (0 past the run count).
+__global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__ run_g,
+                                                    const uint16_t *__restrict__ run_box,
+                                                    const BoxDev *__restrict__ boxes,
+                                                    const DevScal *__restrict__ sc, int64_t cap,
                                                     const uint32_t *__restrict__ top_first,
                                                     const uint32_t *__restrict__ top_end,
                                                     uint32_t dense_min,
                                                     uint32_t *__restrict__ flag) {
-  const uint32_t R = *nruns;
-  for (int64_t r = gtid(); r < R; r += gstride()) {
-    const uint64_t t = top_of_run(g, run_g[r]);
-    flag[r] = (top_first[t] == (uint32_t)r && top_end[t] - top_first[t] > dense_min) ? 1u : 0u;
+  const uint32_t R = sc->R;
+  for (int64_t r = gtid(); r < cap; r += gstride()) {
+    uint32_t f = 0;
+    if (r < R) {
+      const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
+      f = (top_first[t] == (uint32_t)r && top_end[t] - top_first[t] > dense_min) ? 1u : 0u;
+    }
+    flag[r] = f;
   }
 }
 
-__global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ run_g, Geom g,
-                                                   const uint32_t *__restrict__ nruns,
+// Fine-cell maps of the dense top cells (the first nd_cap of them; a dense
+// top cell without a map is scanned instead, which is slower but exact).
+__global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ run_g,
+                                                   const uint16_t *__restrict__ run_box,
+                                                   const BoxDev *__restrict__ boxes,
+                                                   DevScal *sc, uint64_t k3all,
                                                    const uint32_t *__restrict__ top_first,
                                                    const uint32_t *__restrict__ top_end,
                                                    const uint32_t *__restrict__ dflag,
                                                    const uint32_t *__restrict__ dscan,
-                                                   uint32_t dense_min,
+                                                   uint32_t dense_min, uint32_t nd_cap,
                                                    uint32_t *__restrict__ top_slot,
                                                    uint2 *__restrict__ dense_range,
                                                    int32_t *__restrict__ maps) {
-  const uint32_t R = *nruns;
-  const int k = g.k;
+  const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
+    const BoxDev &bx = boxes[run_box[r]];
     const uint64_t pg = run_g[r];
-    const uint64_t t = top_of_run(g, pg);
+    const uint64_t t = top_of_run(bx, pg);
     const uint32_t f = top_first[t];
     if (top_end[t] - f <= dense_min) continue;
-    const uint32_t slot = dscan[f];  // the first run of the cell carries the slot
+    const uint32_t slot = dscan[f];  // the first fine cell of the top cell carries the slot
+    if (slot >= nd_cap) continue;
     if (dflag[r]) {
       top_slot[t] = slot;
       dense_range[slot] = make_uint2(f, top_end[t]);
     }
+    const int k = bx.g.k;
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const uint64_t sub = ((uint64_t)(gz % k) * k + (gy % k)) * k + (gx % k);
-    maps[(uint64_t)slot * g.k3 + sub] = (int32_t)r;
+    maps[(uint64_t)slot * k3all + sub] = (int32_t)r;
   }
 }
 
+__global__ void k_clamp_dense(DevScal *sc, uint32_t nd_cap) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && sc->nd > nd_cap) atomicOr(&sc->overflow, 2u);
+}
+
 __global__ void __launch_bounds__(kT) k_iota(uint32_t *__restrict__ a,
-                                             const uint32_t *__restrict__ nruns) {
-  const uint32_t R = *nruns;
+                                             const DevScal *__restrict__ sc) {
+  const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) a[r] = (uint32_t)r;
 }
 
@@ -323,10 +439,34 @@ __device__ __forceinline__ double box_dist2(const Geom &g, double x, double y, d
   return ex * ex + ey * ey + ez * ez;
 }
 
-// Per-thread tallies of the befriending kernel, flushed once per warp.
+// Per-thread tallies of the befriending kernels, flushed once per warp.
 struct BfStats {
   unsigned long long tests = 0, rechecks = 0, cand = 0, skips = 0, unions = 0, steps = 0;
   unsigned long long scan = 0, window = 0;
+
+  __device__ void flush(Counters *ctr) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      tests += __shfl_down_sync(0xffffffffu, tests, d);
+      rechecks += __shfl_down_sync(0xffffffffu, rechecks, d);
+      cand += __shfl_down_sync(0xffffffffu, cand, d);
+      skips += __shfl_down_sync(0xffffffffu, skips, d);
+      unions += __shfl_down_sync(0xffffffffu, unions, d);
+      steps += __shfl_down_sync(0xffffffffu, steps, d);
+      scan += __shfl_down_sync(0xffffffffu, scan, d);
+      window += __shfl_down_sync(0xffffffffu, window, d);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (tests) atomicAdd(&ctr->pair_tests, tests);
+      if (rechecks) atomicAdd(&ctr->rechecks, rechecks);
+      if (cand) atomicAdd(&ctr->cand_pairs, cand);
+      if (skips) atomicAdd(&ctr->root_skips, skips);
+      if (unions) atomicAdd(&ctr->unions, unions);
+      if (steps) atomicAdd(&ctr->find_steps, steps);
+      if (scan) atomicAdd(&ctr->scan_iters, scan);
+      if (window) atomicAdd(&ctr->window_iters, window);
+    }
+  }
 };
 
 // Whether any particle of fine cell a (particles [sa, ea)) is linked to any
@@ -417,30 +557,32 @@ __device__ __forceinline__ void lunion(uint32_t *lp, uint32_t a, uint32_t b, Cou
 // joined with a shared-memory union-find (neighbours found through the top
 // cell's fine-cell map), near pairs before far ones; then every fine cell's
 // global parent is set to its local root.  Links that cross the top cell's
-// faces are left to the global passes.
+// faces are left to the global passes.  CTAs take top cells from an atomic
+// counter: their sizes differ widely.
 template <class PT, bool FP32>
 __global__ void __launch_bounds__(128) k_befriend_dense(
-    Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
-    const uint2 *__restrict__ dense_range, const uint32_t *__restrict__ ndense, uint32_t *next,
+    const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
+    const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
+    const uint2 *__restrict__ dense_range, DevScal *sc, uint32_t nd_cap,
     const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos, uint32_t *parent,
     Counters *ctr) {
   extern __shared__ uint32_t lpar[];
   __shared__ uint32_t s_slot;
-  const uint32_t nd = *ndense;
-  const int k = g.k, W = g.W;
+  const uint32_t nd = min(sc->nd, nd_cap);
   BfStats st;
   while (true) {
-    // top cells are taken from an atomic counter: their sizes differ widely
-    if (threadIdx.x == 0) s_slot = atomicAdd(next, 1u);
+    if (threadIdx.x == 0) s_slot = atomicAdd(&sc->next_dense, 1u);
     __syncthreads();
     const uint32_t slot = s_slot;
     __syncthreads();
     if (slot >= nd) break;
     const uint2 fr = dense_range[slot];
     const uint32_t f = fr.x, n = fr.y - fr.x;
+    const Geom &g = boxes[run_box[f]].g;
+    const int k = g.k, W = g.W;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) lpar[i] = i;
     __syncthreads();
-    const int32_t *map = maps + (uint64_t)slot * g.k3;
+    const int32_t *map = maps + (uint64_t)slot * k3all;
     for (int pass = 0; pass < 2; pass++) {
       for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t a = f + i;
@@ -478,25 +620,11 @@ __global__ void __launch_bounds__(128) k_befriend_dense(
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) parent[f + i] = f + lfind(lpar, i);
     __syncthreads();
   }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    st.tests += __shfl_down_sync(0xffffffffu, st.tests, d);
-    st.rechecks += __shfl_down_sync(0xffffffffu, st.rechecks, d);
-    st.cand += __shfl_down_sync(0xffffffffu, st.cand, d);
-    st.skips += __shfl_down_sync(0xffffffffu, st.skips, d);
-    st.unions += __shfl_down_sync(0xffffffffu, st.unions, d);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (st.tests) atomicAdd(&ctr->pair_tests, st.tests);
-    if (st.rechecks) atomicAdd(&ctr->rechecks, st.rechecks);
-    if (st.cand) atomicAdd(&ctr->cand_pairs, st.cand);
-    if (st.skips) atomicAdd(&ctr->root_skips, st.skips);
-    if (st.unions) atomicAdd(&ctr->unions, st.unions);
-  }
+  st.flush(ctr);
 }
 
-// Whether fine cell a's neighbour top cell in direction (ox, oy, oz) lies
-// within W fine cells of a (s = a's fine coordinates inside its top cell).
+// Whether fine cell a's neighbour top cell in direction o lies within W fine
+// cells of a (s = a's fine coordinate inside its top cell).
 __device__ __forceinline__ bool reaches(int s, int o, int k, int W) {
   return o == 0 || (o > 0 ? s >= k - W : s <= W - 1);
 }
@@ -505,26 +633,28 @@ __device__ __forceinline__ bool reaches(int s, int o, int k, int W) {
 // unordered pair is visited once) within W fine cells on every axis; they
 // live in a's top cell (after a) and the 13 forward top cells.
 //
-// Fast path, one thread per fine cell: the 14 top-cell ranges are loaded at
-// once; when no range holds more than kSimple candidate cells (the common
-// case away from clumps), the first of each is loaded at once too and the
-// cell is finished in two L2 round trips.  Other cells are queued for the
-// warp path below.
+// Fast path, one thread per fine cell: the ranges of the top cells a can
+// reach are loaded at once; when none holds more than kSimple candidate cells
+// (the common case away from clumps), the first of each is loaded at once too
+// and the cell is finished in two L2 round trips.  Other cells are queued for
+// the warp path below.
 constexpr uint32_t kSimple = 2;
 
 template <class PT, bool FP32>
 __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
-    Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
-    const uint32_t *__restrict__ nruns, const uint32_t *__restrict__ top_first,
-    const uint32_t *__restrict__ top_end, uint32_t dense_min,
-    const SPos<PT> *__restrict__ spos, uint32_t *parent, uint32_t *__restrict__ queue,
-    uint32_t *qcount, Counters *ctr) {
-  const uint32_t R = *nruns;
-  const int k = g.k, W = g.W;
+    const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box,
+    const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g, DevScal *sc,
+    const uint32_t *__restrict__ top_first, const uint32_t *__restrict__ top_end,
+    const uint32_t *__restrict__ top_slot, const SPos<PT> *__restrict__ spos, uint32_t *parent,
+    uint32_t *__restrict__ queue, Counters *ctr) {
+  const uint32_t R = sc->R;
   const int lane = threadIdx.x & 31;
   BfStats st;
   for (int64_t ai = gtid(); ai < R; ai += gstride()) {
     const uint32_t a = (uint32_t)ai;
+    const BoxDev &bx = boxes[run_box[a]];
+    const Geom &g = bx.g;
+    const int k = g.k, W = g.W;
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const int tx = gx / k, ty = gy / k, tz = gz / k;
@@ -537,12 +667,12 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
       const bool in = !(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]) &&
                       reaches(sx, kFwd[nb][0], k, W) && reaches(sy, kFwd[nb][1], k, W) &&
                       reaches(sz, kFwd[nb][2], k, W);
-      const uint64_t tb = in ? ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux : 0;
+      const uint64_t tb = in ? bx.top_base + ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux : 0;
       const uint32_t f = in ? top_first[tb] : 0u, e = in ? top_end[tb] : 0u;
       R0[nb] = nb == 0 ? a + 1 : f;
       NN[nb] = e > R0[nb] ? e - R0[nb] : 0u;
       // pairs inside a dense top cell are joined by k_befriend_dense
-      if (nb == 0 && e - f > dense_min) NN[nb] = 0u;
+      if (nb == 0 && in && top_slot[tb] != kNone) NN[nb] = 0u;
     }
     bool simple = true;
 #pragma unroll
@@ -552,7 +682,7 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
     if (qmask) {
       const int leader = __ffs(qmask) - 1;
       uint32_t base = 0;
-      if (lane == leader) base = atomicAdd(qcount, (uint32_t)__popc(qmask));
+      if (lane == leader) base = atomicAdd(&sc->qcount, (uint32_t)__popc(qmask));
       base = __shfl_sync(active, base, leader);
       if (!simple) queue[base + __popc(qmask & ((1u << lane) - 1u))] = a;
     }
@@ -565,58 +695,41 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
     for (int nb = 0; nb < 14; nb++) {
       for (uint32_t q = 0; q < NN[nb]; q++) {
         const uint64_t qg = q == 0 ? Q[nb] : run_g[R0[nb] + q];
-        const int bx = (int)(qg & kM21), by = (int)((qg >> 21) & kM21), bz = (int)(qg >> 42);
+        const int bx2 = (int)(qg & kM21), by2 = (int)((qg >> 21) & kM21), bz2 = (int)(qg >> 42);
         st.scan++;
-        if (max(abs(bx - gx), max(abs(by - gy), abs(bz - gz))) > W) continue;
+        if (max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz))) > W) continue;
         if (ra == 0xffffffffu) {
           ra = __ldcg(parent + a);
           sa = run_start[a];
           ea = run_start[a + 1];
         }
-        try_link<PT, FP32>(g, a, ra, R0[nb] + q, bx, by, bz, sa, ea, run_start, spos, parent,
+        try_link<PT, FP32>(g, a, ra, R0[nb] + q, bx2, by2, bz2, sa, ea, run_start, spos, parent,
                            ctr, st);
       }
     }
   }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    st.tests += __shfl_down_sync(0xffffffffu, st.tests, d);
-    st.rechecks += __shfl_down_sync(0xffffffffu, st.rechecks, d);
-    st.cand += __shfl_down_sync(0xffffffffu, st.cand, d);
-    st.skips += __shfl_down_sync(0xffffffffu, st.skips, d);
-    st.unions += __shfl_down_sync(0xffffffffu, st.unions, d);
-    st.steps += __shfl_down_sync(0xffffffffu, st.steps, d);
-    st.scan += __shfl_down_sync(0xffffffffu, st.scan, d);
-  }
-  if (lane == 0) {
-    if (st.tests) atomicAdd(&ctr->pair_tests, st.tests);
-    if (st.rechecks) atomicAdd(&ctr->rechecks, st.rechecks);
-    if (st.cand) atomicAdd(&ctr->cand_pairs, st.cand);
-    if (st.skips) atomicAdd(&ctr->root_skips, st.skips);
-    if (st.unions) atomicAdd(&ctr->unions, st.unions);
-    if (st.steps) atomicAdd(&ctr->find_steps, st.steps);
-    if (st.scan) atomicAdd(&ctr->scan_iters, st.scan);
-  }
+  st.flush(ctr);
 }
 
 // Warp path, one warp per queued fine cell a.  Lanes 0..13 fetch the 14
 // top-cell ranges at once; the candidate slots of all 14 (fine cells of small
-// top cells, map slots of the window in dense ones) are then flattened and
+// top cells, map slots of the window in mapped ones) are then flattened and
 // taken 32 at a time, so a cell costs a few L2 round trips instead of one per
-// slot.  Warps take cells from `next` (an atomic counter) as they finish, so
-// a few expensive cells do not hold back a whole static share.  PHASE 0
-// visits the candidates within one fine cell, PHASE 1 the farther ones, so
-// that a dense neighbourhood is joined (and compressed) before its far pairs
-// are tried and most of those become root skips.
+// slot.  Warps take cells from an atomic counter as they finish, so a few
+// expensive cells do not hold back a whole static share.  PHASE 0 visits the
+// candidates within one fine cell, PHASE 1 the farther ones, so that a dense
+// neighbourhood is joined (and compressed) before its far pairs are tried and
+// most of those become root skips.
 template <class PT, bool FP32, int PHASE>
 __global__ void __launch_bounds__(kT) k_befriend(
-    Geom g, const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
-    const uint32_t *__restrict__ queue, const uint32_t *__restrict__ qcount, uint32_t *next,
-    const uint32_t *__restrict__ top_first, const uint32_t *__restrict__ top_end,
-    const uint32_t *__restrict__ top_slot, const int32_t *__restrict__ maps, uint32_t dense_min,
-    const SPos<PT> *__restrict__ spos, uint32_t *parent, Counters *ctr) {
-  const uint32_t NQ = *qcount;
-  const int k = g.k, W = g.W;
+    const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
+    const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
+    const uint32_t *__restrict__ queue, DevScal *sc, const uint32_t *__restrict__ top_first,
+    const uint32_t *__restrict__ top_end, const uint32_t *__restrict__ top_slot,
+    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos, uint32_t *parent,
+    Counters *ctr) {
+  const uint32_t NQ = sc->qcount;
+  uint32_t *next = PHASE == 0 ? &sc->next0 : &sc->next1;
   const int lane = threadIdx.x & 31;
   BfStats st;
   while (true) {
@@ -625,6 +738,9 @@ __global__ void __launch_bounds__(kT) k_befriend(
     qi = __shfl_sync(0xffffffffu, qi, 0);
     if (qi >= NQ) break;
     const uint32_t a = queue[qi];
+    const BoxDev &bx = boxes[run_box[a]];
+    const Geom &g = bx.g;
+    const int k = g.k, W = g.W;
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
     const int tx = gx / k, ty = gy / k, tz = gz / k;
@@ -639,27 +755,27 @@ __global__ void __launch_bounds__(kT) k_befriend(
       if (!(ux < 0 || uy < 0 || ux >= g.T[0] || uy >= g.T[1] || uz >= g.T[2]) &&
           reaches(sx, kFwd[lane][0], k, W) && reaches(sy, kFwd[lane][1], k, W) &&
           reaches(sz, kFwd[lane][2], k, W)) {
-        const uint64_t tb = ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux;
+        const uint64_t tb = bx.top_base + ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux;
         const uint32_t f = top_first[tb], e = top_end[tb];
+        const uint32_t slot = top_slot[tb];
         r0 = lane == 0 ? a + 1 : f;
-        // pairs inside a dense top cell are joined by k_befriend_dense
-        if (lane == 0 && e - f > dense_min) r0 = e;
+        // pairs inside a mapped top cell are joined by k_befriend_dense
+        if (lane == 0 && slot != kNone) r0 = e;
         if (r0 < e) {
-          if (e - f <= dense_min) {
+          if (slot == kNone) {
             nsparse = e - r0;
           } else {
             x0 = max(gx - W, ux * k);
             const int x1 = min(gx + W, ux * k + k - 1);
             y0 = max(gy - W, uy * k);
             const int y1 = min(gy + W, uy * k + k - 1);
-            // in a's own top cell only rows at or after a's hold cells b > a
-            z0 = max(lane == 0 ? gz : gz - W, uz * k);
+            z0 = max(gz - W, uz * k);
             const int z1 = min(gz + W, uz * k + k - 1);
             if (x1 >= x0 && y1 >= y0 && z1 >= z0) {
               nx = x1 - x0 + 1;
               ny = y1 - y0 + 1;
               nslots = (uint32_t)(nx * ny * (z1 - z0 + 1));
-              mapbase = top_slot[tb];
+              mapbase = slot;
               ox = ux * k;
               oy = uy * k;
               oz = uz * k;
@@ -695,58 +811,37 @@ __global__ void __launch_bounds__(kT) k_befriend(
       if (j >= total) continue;
       const uint32_t off = j - l_excl;
       uint32_t r;
-      int bx, by, bz;
+      int bx2, by2, bz2;
       if (off < l_ns) {
         st.scan++;
         r = l_r0 + off;
         const uint64_t qg = run_g[r];
-        bx = (int)(qg & kM21);
-        by = (int)((qg >> 21) & kM21);
-        bz = (int)(qg >> 42);
-        if (max(abs(bx - gx), max(abs(by - gy), abs(bz - gz))) > W) continue;
+        bx2 = (int)(qg & kM21);
+        by2 = (int)((qg >> 21) & kM21);
+        bz2 = (int)(qg >> 42);
+        if (max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz))) > W) continue;
       } else {
         st.window++;
         const uint32_t sl = off - l_ns;
-        bx = l_x0 + (int)(sl % (uint32_t)l_nx);
-        by = l_y0 + (int)((sl / (uint32_t)l_nx) % (uint32_t)l_ny);
-        bz = l_z0 + (int)(sl / (uint32_t)(l_nx * l_ny));
-        const int32_t rr =
-            maps[(uint64_t)l_map * g.k3 + (uint64_t)(((bz - l_oz) * k + (by - l_oy)) * k + (bx - l_ox))];
+        bx2 = l_x0 + (int)(sl % (uint32_t)l_nx);
+        by2 = l_y0 + (int)((sl / (uint32_t)l_nx) % (uint32_t)l_ny);
+        bz2 = l_z0 + (int)(sl / (uint32_t)(l_nx * l_ny));
+        const int32_t rr = maps[(uint64_t)l_map * k3all +
+                                (uint64_t)(((bz2 - l_oz) * k + (by2 - l_oy)) * k + (bx2 - l_ox))];
         if (rr < 0 || (uint32_t)rr < l_r0) continue;
         r = (uint32_t)rr;
       }
-      const int cheb = max(abs(bx - gx), max(abs(by - gy), abs(bz - gz)));
+      const int cheb = max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz)));
       if ((PHASE == 0 && cheb > 1) || (PHASE == 1 && cheb <= 1)) continue;
-      try_link<PT, FP32>(g, a, ra, r, bx, by, bz, sa, ea, run_start, spos, parent, ctr, st);
+      try_link<PT, FP32>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, parent, ctr, st);
     }
   }
-  // one atomic per warp for the counters
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    st.tests += __shfl_down_sync(0xffffffffu, st.tests, d);
-    st.rechecks += __shfl_down_sync(0xffffffffu, st.rechecks, d);
-    st.cand += __shfl_down_sync(0xffffffffu, st.cand, d);
-    st.skips += __shfl_down_sync(0xffffffffu, st.skips, d);
-    st.unions += __shfl_down_sync(0xffffffffu, st.unions, d);
-    st.steps += __shfl_down_sync(0xffffffffu, st.steps, d);
-    st.scan += __shfl_down_sync(0xffffffffu, st.scan, d);
-    st.window += __shfl_down_sync(0xffffffffu, st.window, d);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (st.tests) atomicAdd(&ctr->pair_tests, st.tests);
-    if (st.rechecks) atomicAdd(&ctr->rechecks, st.rechecks);
-    if (st.cand) atomicAdd(&ctr->cand_pairs, st.cand);
-    if (st.skips) atomicAdd(&ctr->root_skips, st.skips);
-    if (st.unions) atomicAdd(&ctr->unions, st.unions);
-    if (st.steps) atomicAdd(&ctr->find_steps, st.steps);
-    if (st.scan) atomicAdd(&ctr->scan_iters, st.scan);
-    if (st.window) atomicAdd(&ctr->window_iters, st.window);
-  }
+  st.flush(ctr);
 }
 
 __global__ void __launch_bounds__(kT) k_compress(uint32_t *parent,
-                                                 const uint32_t *__restrict__ nruns) {
-  const uint32_t R = *nruns;
+                                                 const DevScal *__restrict__ sc) {
+  const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) parent[r] = uf_find(parent, (uint32_t)r);
 }
 
@@ -799,9 +894,11 @@ __device__ __forceinline__ bool warp_segments_count_min(uint32_t key, uint32_t &
 // Group size and head (lowest processing index) per root cell.
 __global__ void __launch_bounds__(kT) k_group_count(const uint32_t *__restrict__ run_of,
                                                     const uint32_t *__restrict__ parent,
-                                                    const uint32_t *__restrict__ perm, int64_t np,
+                                                    const uint32_t *__restrict__ perm,
+                                                    const DevScal *__restrict__ sc,
                                                     uint32_t *__restrict__ count,
                                                     uint32_t *__restrict__ head) {
+  const int64_t np = sc->np;
   const int64_t n_iter = (np + 31) / 32 * 32;
   for (int64_t i = gtid(); i < n_iter; i += gstride()) {
     const bool valid = i < np;
@@ -816,17 +913,25 @@ __global__ void __launch_bounds__(kT) k_group_count(const uint32_t *__restrict__
   }
 }
 
+// Candidate flags (0 past the run count): roots with at least Nphalomin
+// members (FOF.c:202).
 __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ parent,
                                                    const uint32_t *__restrict__ count,
-                                                   const uint32_t *__restrict__ nruns,
-                                                   double nphalomin, uint32_t *__restrict__ flag,
+                                                   const uint16_t *__restrict__ run_box,
+                                                   const BoxDev *__restrict__ boxes,
+                                                   const DevScal *__restrict__ sc, int64_t cap,
+                                                   uint32_t *__restrict__ flag,
                                                    unsigned long long *ngroups) {
-  const uint32_t R = *nruns;
+  const uint32_t R = sc->R;
   unsigned long long roots = 0;
-  for (int64_t r = gtid(); r < R; r += gstride()) {
-    const bool root = parent[r] == (uint32_t)r;
-    roots += root;
-    flag[r] = (root && !((double)count[r] < nphalomin)) ? 1u : 0u;  // FOF.c:202
+  for (int64_t r = gtid(); r < cap; r += gstride()) {
+    uint32_t f = 0;
+    if (r < R) {
+      const bool root = parent[r] == (uint32_t)r;
+      roots += root;
+      f = (root && !((double)count[r] < boxes[run_box[r]].g.nphalomin)) ? 1u : 0u;
+    }
+    flag[r] = f;
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) roots += __shfl_down_sync(0xffffffffu, roots, d);
@@ -835,10 +940,10 @@ __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ 
 
 __global__ void __launch_bounds__(kT) k_cand_list(const uint32_t *__restrict__ flag,
                                                   const uint32_t *__restrict__ scan,
-                                                  const uint32_t *__restrict__ nruns,
+                                                  const DevScal *__restrict__ sc,
                                                   uint32_t *__restrict__ cand_of_root,
                                                   uint32_t *__restrict__ cand_root) {
-  const uint32_t R = *nruns;
+  const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
     if (!flag[r]) continue;
     cand_of_root[r] = scan[r];
@@ -849,12 +954,14 @@ __global__ void __launch_bounds__(kT) k_cand_list(const uint32_t *__restrict__ f
 // Property sums per candidate halo, in double as Output_Halos does
 // (FOF.c:806-832): 6 first moments, then 6 position and 6 velocity second
 // moments when INERTIA / DISPERSION are asked for.
-template <class PT, class VT, int NS>
+template <class PT, int NS>
 __global__ void __launch_bounds__(kT) k_group_sums(
     const uint32_t *__restrict__ run_of, const uint32_t *__restrict__ parent,
-    const uint32_t *__restrict__ cand_of_root, const SPos<PT> *__restrict__ spos,
-    const VT *__restrict__ vel, int64_t np, Geom g, double *__restrict__ sums,
+    const uint32_t *__restrict__ cand_of_root, const uint16_t *__restrict__ run_box,
+    const BoxDev *__restrict__ boxes, const SPos<PT> *__restrict__ spos,
+    const DevScal *__restrict__ sc, int props, double *__restrict__ sums,
     uint32_t *__restrict__ warn) {
+  const int64_t np = sc->np;
   const int64_t n_iter = (np + 31) / 32 * 32;
   for (int64_t i = gtid(); i < n_iter; i += gstride()) {
     uint32_t ci = kNone;
@@ -862,15 +969,25 @@ __global__ void __launch_bounds__(kT) k_group_sums(
 #pragma unroll
     for (int c = 0; c < NS; c++) v[c] = 0.0;
     if (i < np) {
-      ci = cand_of_root[parent[run_of[i]]];
+      const uint32_t run = run_of[i];
+      ci = cand_of_root[parent[run]];
       if (ci != kNone) {
+        const BoxDev &bx = boxes[run_box[run]];
+        const Geom &g = bx.g;
         const SPos<PT> p = spos[i];
         const double x = (double)p.x, y = (double)p.y, z = (double)p.z;
-        const double vx = (double)vel[3 * (uint64_t)p.src], vy = (double)vel[3 * (uint64_t)p.src + 1],
-                     vz = (double)vel[3 * (uint64_t)p.src + 2];
+        const uint64_t li = 3 * ((uint64_t)p.src - bx.in_base);
+        double vx, vy, vz;
+        if (bx.vel_f64) {
+          const double *vel = static_cast<const double *>(bx.vel);
+          vx = vel[li]; vy = vel[li + 1]; vz = vel[li + 2];
+        } else {
+          const float *vel = static_cast<const float *>(bx.vel);
+          vx = (double)vel[li]; vy = (double)vel[li + 1]; vz = (double)vel[li + 2];
+        }
         v[0] = x; v[1] = y; v[2] = z; v[3] = vx; v[4] = vy; v[5] = vz;
         if constexpr (NS >= 12) {
-          if (g.props & 1) {
+          if (props & 1) {
             v[6] = __dmul_rn(x, x); v[7] = __dmul_rn(y, y); v[8] = __dmul_rn(z, z);
             v[9] = __dmul_rn(x, y); v[10] = __dmul_rn(x, z); v[11] = __dmul_rn(y, z);
           }
@@ -879,7 +996,7 @@ __global__ void __launch_bounds__(kT) k_group_sums(
           v[12] = __dmul_rn(vx, vx); v[13] = __dmul_rn(vy, vy); v[14] = __dmul_rn(vz, vz);
           v[15] = __dmul_rn(vx, vy); v[16] = __dmul_rn(vx, vz); v[17] = __dmul_rn(vy, vz);
         } else if constexpr (NS >= 12) {
-          if (!(g.props & 1)) {
+          if (!(props & 1)) {
             v[6] = __dmul_rn(vx, vx); v[7] = __dmul_rn(vy, vy); v[8] = __dmul_rn(vz, vz);
             v[9] = __dmul_rn(vx, vy); v[10] = __dmul_rn(vx, vz); v[11] = __dmul_rn(vy, vz);
           }
@@ -901,21 +1018,28 @@ __global__ void __launch_bounds__(kT) k_group_sums(
 }
 
 // Ownership (Checkhalo, FOF.c:394-401): centre of mass by division, kept iff
-// inside [lo, hi) on every axis.
+// inside [lo, hi) on every axis.  Flags are 0 past the candidate count.
 template <int NS>
 __global__ void __launch_bounds__(kT) k_owned(const double *__restrict__ sums,
                                               const uint32_t *__restrict__ cand_root,
                                               const uint32_t *__restrict__ count,
-                                              const uint32_t *__restrict__ ncand, Geom g,
+                                              const uint16_t *__restrict__ run_box,
+                                              const BoxDev *__restrict__ boxes,
+                                              const DevScal *__restrict__ sc, int64_t cap,
                                               uint32_t *__restrict__ own) {
-  const uint32_t nc = *ncand;
-  for (int64_t c = gtid(); c < nc; c += gstride()) {
-    const double n = (double)count[cand_root[c]];
-    bool ok = true;
+  const uint32_t nc = sc->nc;
+  for (int64_t c = gtid(); c < cap; c += gstride()) {
+    bool ok = false;
+    if (c < nc) {
+      const uint32_t root = cand_root[c];
+      const Geom &g = boxes[run_box[root]].g;
+      const double n = (double)count[root];
+      ok = true;
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const double com = __ddiv_rn(sums[(uint64_t)c * NS + a], n);
-      ok &= (com >= g.lo[a]) && (com < g.hi[a]);
+      for (int a = 0; a < 3; a++) {
+        const double com = __ddiv_rn(sums[(uint64_t)c * NS + a], n);
+        ok &= (com >= g.lo[a]) && (com < g.hi[a]);
+      }
     }
     own[c] = ok ? 1u : 0u;
   }
@@ -925,10 +1049,10 @@ __global__ void __launch_bounds__(kT) k_own_list(const uint32_t *__restrict__ ow
                                                  const uint32_t *__restrict__ own_scan,
                                                  const uint32_t *__restrict__ cand_root,
                                                  const uint32_t *__restrict__ head,
-                                                 const uint32_t *__restrict__ ncand,
+                                                 const DevScal *__restrict__ sc,
                                                  uint32_t *__restrict__ okeys,
                                                  uint32_t *__restrict__ ovals) {
-  const uint32_t nc = *ncand;
+  const uint32_t nc = sc->nc;
   for (int64_t c = gtid(); c < nc; c += gstride()) {
     if (!own[c]) continue;
     okeys[own_scan[c]] = head[cand_root[c]];
@@ -938,30 +1062,35 @@ __global__ void __launch_bounds__(kT) k_own_list(const uint32_t *__restrict__ ow
 
 // Halo records (Output_Halos, FOF.c:836-872): means by the reciprocal of n,
 // second-moment combinations as written there, all in double, then float.
+// The head is reported as an index into the box's own processing order.
 template <int NS>
 __global__ void __launch_bounds__(kT) k_catalog(const uint32_t *__restrict__ okeys,
                                                 const uint32_t *__restrict__ ovals,
-                                                const uint32_t *__restrict__ nown,
+                                                const DevScal *__restrict__ sc,
                                                 const double *__restrict__ sums,
                                                 const uint32_t *__restrict__ cand_root,
                                                 const uint32_t *__restrict__ count,
-                                                const uint32_t *__restrict__ warn, Geom g,
-                                                float *__restrict__ props,
+                                                const uint32_t *__restrict__ warn,
+                                                const uint16_t *__restrict__ run_box,
+                                                uint32_t *__restrict__ boxd, int nbox, int props,
+                                                int hs, float *__restrict__ out_props,
                                                 uint32_t *__restrict__ head_out,
                                                 uint32_t *__restrict__ cat_of_cand,
                                                 unsigned long long *n_warn) {
-  const uint32_t nh = *nown;
+  const uint32_t nh = sc->nh;
   for (int64_t h = gtid(); h < nh; h += gstride()) {
     const uint32_t c = ovals[h];
-    const uint32_t n = count[cand_root[c]];
+    const uint32_t root = cand_root[c];
+    const uint32_t n = count[root];
+    const int b = run_box[root];
     const double *s = sums + (uint64_t)c * NS;
     const double inv = __ddiv_rn(1.0, (double)n);
-    float *rec = props + (uint64_t)h * g.hs;
+    float *rec = out_props + (uint64_t)h * hs;
     int o = 0;
     rec[o++] = (float)n;
     for (int q = 0; q < 6; q++) rec[o++] = __double2float_rn(__dmul_rn(s[q], inv));
     int m = 6;
-    if (g.props & 1) {
+    if (props & 1) {
       const double xx = s[m], yy = s[m + 1], zz = s[m + 2], xy = s[m + 3], xz = s[m + 4],
                    yz = s[m + 5];
       const double X = s[0], Y = s[1], Z = s[2];
@@ -973,7 +1102,7 @@ __global__ void __launch_bounds__(kT) k_catalog(const uint32_t *__restrict__ oke
       rec[o++] = __double2float_rn(__dsub_rn(__dmul_rn(__dmul_rn(inv, Y), Z), yz));
       m += 6;
     }
-    if (g.props & 2) {
+    if (props & 2) {
       const double VX = s[3], VY = s[4], VZ = s[5];
       const double A[6] = {s[m], s[m + 1], s[m + 2], s[m + 3], s[m + 4], s[m + 5]};
       const double P[6] = {__dmul_rn(VX, VX), __dmul_rn(VY, VY), __dmul_rn(VZ, VZ),
@@ -981,23 +1110,37 @@ __global__ void __launch_bounds__(kT) k_catalog(const uint32_t *__restrict__ oke
       for (int q = 0; q < 6; q++)
         rec[o++] = __double2float_rn(__dmul_rn(__dsub_rn(A[q], __dmul_rn(P[q], inv)), inv));
     }
-    head_out[h] = okeys[h];
+    head_out[h] = okeys[h] - boxd[4 * nbox + b];
     cat_of_cand[c] = (uint32_t)h;
+    atomicAdd(&boxd[5 * nbox + b], 1u);
     if (warn[c]) atomicAdd(n_warn, 1ull);
+  }
+}
+
+// First catalog index of each box: owned halos are sorted by processing
+// index, which numbers the boxes one after another.
+__global__ void k_halo_base(uint32_t *boxd, int nbox) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t acc = 0;
+  for (int b = 0; b < nbox; b++) {
+    boxd[6 * nbox + b] = acc;
+    acc += boxd[5 * nbox + b];
   }
 }
 
 // Membership per input particle: the owned halo holding it (or one of its
 // images) -- the lowest catalog index when a halo wider than the ghost shell
-// leaves two owned copies -- then, in a second pass, the processing index
-// of that copy and its stored coordinates.
+// leaves two owned copies -- then, in a second pass, the processing index of
+// that copy (in its box's numbering) and its stored coordinates.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_member(const uint32_t *__restrict__ run_of,
                                                const uint32_t *__restrict__ parent,
                                                const uint32_t *__restrict__ cand_of_root,
                                                const uint32_t *__restrict__ cat_of_cand,
-                                               const SPos<PT> *__restrict__ spos, int64_t np,
+                                               const SPos<PT> *__restrict__ spos,
+                                               const DevScal *__restrict__ sc,
                                                unsigned long long *__restrict__ member) {
+  const int64_t np = sc->np;
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const uint32_t ci = cand_of_root[parent[run_of[i]]];
     if (ci == kNone) continue;
@@ -1011,17 +1154,20 @@ template <class PT>
 __global__ void __launch_bounds__(kT) k_member_copy(
     const uint32_t *__restrict__ run_of, const uint32_t *__restrict__ parent,
     const uint32_t *__restrict__ cand_of_root, const uint32_t *__restrict__ cat_of_cand,
-    const SPos<PT> *__restrict__ spos, const uint32_t *__restrict__ perm, int64_t np,
-    const unsigned long long *__restrict__ member, uint32_t *__restrict__ member_proc,
-    float *__restrict__ member_pos, Counters *ctr) {
+    const uint16_t *__restrict__ run_box, const uint32_t *__restrict__ boxd, int nbox,
+    const SPos<PT> *__restrict__ spos, const uint32_t *__restrict__ perm,
+    const DevScal *__restrict__ sc, const unsigned long long *__restrict__ member,
+    uint32_t *__restrict__ member_proc, float *__restrict__ member_pos, Counters *ctr) {
+  const int64_t np = sc->np;
   for (int64_t i = gtid(); i < np; i += gstride()) {
-    const uint32_t ci = cand_of_root[parent[run_of[i]]];
+    const uint32_t run = run_of[i];
+    const uint32_t ci = cand_of_root[parent[run]];
     if (ci == kNone) continue;
     const uint32_t h = cat_of_cand[ci];
     if (h == kNone) continue;
     const SPos<PT> p = spos[i];
     if (member[p.src] == (unsigned long long)h) {
-      member_proc[p.src] = perm[i];
+      member_proc[p.src] = perm[i] - boxd[4 * nbox + run_box[run]];
       member_pos[3 * (uint64_t)p.src] = (float)p.x;
       member_pos[3 * (uint64_t)p.src + 1] = (float)p.y;
       member_pos[3 * (uint64_t)p.src + 2] = (float)p.z;
@@ -1040,17 +1186,16 @@ int bits_for(uint64_t v) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Host side of one run.
+// Host side.
 // ---------------------------------------------------------------------------
 
-void Plan::setup_geometry(int64_t n_in) {
-  const cmh_fof_params &p = params;
-  Geom &g = geom;
-  g = Geom{};
+Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &ltab,
+                         int64_t n_in, int cell_factor) const {
+  Geom g{};
   double minlink = p.linklength, maxlink = p.linklength;
   if (p.varlink) {
-    minlink = maxlink = ltab_host.empty() ? p.linklength : ltab_host[0];
-    for (double v : ltab_host) {
+    minlink = maxlink = ltab.empty() ? p.linklength : ltab[0];
+    for (double v : ltab) {
       minlink = std::min(minlink, v);
       maxlink = std::max(maxlink, v);
     }
@@ -1084,359 +1229,491 @@ void Plan::setup_geometry(int64_t n_in) {
     if (g.G[a] >= (1 << 21)) fail(CMH_ERR_CAPACITY, "more than 2^21 fine cells along an axis");
     vol *= (g.rmax[a] - g.rmin[a]);
   }
-  int k = p.cell_factor;
+  int k = cell_factor > 0 ? cell_factor : p.cell_factor;
   if (k <= 0) {
     // one top cell per particle on average, as the reference's lcell = L/Px
     const double sep = std::cbrt(vol / std::max<double>((double)n_in, 1.0));
     k = (int)std::lround(sep / g.h);
   }
-  k = std::max(k, g.W);
+  k = std::min(std::max(k, g.W), kMaxCellFactor);
   while (true) {
     uint64_t T = 1;
     for (int a = 0; a < 3; a++) {
       g.T[a] = (g.G[a] + k - 1) / k;
       T *= (uint64_t)g.T[a];
     }
-    const uint64_t k3 = (uint64_t)k * k * k;
-    if (T < (1ull << 31) && (T * k3) < (1ull << 62)) {
+    if (T < (1ull << 31) || k >= kMaxCellFactor) {
+      if (T >= (1ull << 31)) fail(CMH_ERR_CAPACITY, "domain too large for the top-cell grid");
       g.k = k;
-      g.k3 = k3;
-      n_top = T;
-      key_bits = bits_for(T * k3 - 1);
+      g.k3 = (uint64_t)k * k * k;
       break;
     }
     k++;
   }
+  return g;
 }
 
-template <class PT, class VT>
-void Plan::run_typed(const cmh_particles &parts, bool want_member, cudaStream_t s) {
-  const int64_t n = parts.n;
-  const PT *pos = static_cast<const PT *>(parts.pos);
-  const VT *vel = static_cast<const VT *>(parts.vel);
-  Geom &g = geom;
-  stats = cmh_stats{};
-  stats.n_in = n;
-  const long long launches0 = g_launches;
-  CMH_CUDA(cudaEventRecord(ev0, s));
+namespace {
+// Images per input particle expected for a periodic box (the shell's share
+// of the padded volume), with headroom for clustering.
+double image_estimate(const Geom &g, int64_t n) {
+  if (!g.periodic) return 0.0;
+  double f = 1.0;
+  for (int a = 0; a < 3; a++) f *= (g.L[a] + 2 * g.boundary) / g.L[a];
+  return (double)n * (f - 1.0) * 1.5 + 4096.0;
+}
+}  // namespace
 
-  // scalars: [0] n_kept [1] n_images [2] R [3] n_dense [4] n_cand [5] n_own
-  scal.ensure(16 * sizeof(uint32_t));
-  ctr.ensure(sizeof(Counters) + 2 * sizeof(unsigned long long));
-  uint32_t *sc = scal.as<uint32_t>();
+template <class PT>
+void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
+  const int nbox = (int)boxes_host.size();
+  const int64_t n = n_total, npc = np_cap, ncc = nc_cap;
+  DevScal *sc = scal.as<DevScal>();
   Counters *c = ctr.as<Counters>();
   unsigned long long *extra = reinterpret_cast<unsigned long long *>(c + 1);  // ngroups, nwarn
-  CMH_CUDA(cudaMemsetAsync(scal.p, 0, 16 * sizeof(uint32_t), s));
+  uint32_t *boxd = b_boxd.as<uint32_t>();
+  const BoxDev *boxes = b_boxes.as<BoxDev>();
+  auto mark = [&](int q) {
+    if (timed) CMH_CUDA(cudaEventRecord(q < 0 ? ev0 : (q >= 7 ? ev1 : stage_ev[q]), s));
+  };
+  mark(-1);
+  CMH_CUDA(cudaMemsetAsync(scal.p, 0, sizeof(DevScal), s));
   CMH_CUDA(cudaMemsetAsync(ctr.p, 0, sizeof(Counters) + 2 * sizeof(unsigned long long), s));
-  if (g.varlink) fail(CMH_ERR_INVALID_ARGUMENT, "variable linking length is not built yet");
+  CMH_CUDA(cudaMemsetAsync(b_boxd.p, 0, 7 * sizeof(uint32_t) * nbox, s));
 
   // ---- ingest ----
-  const int64_t nn = std::max<int64_t>(n, 1);
-  b_keep.ensure(nn * 4);
-  b_nimg.ensure(nn * 4);
-  b_keep_scan.ensure(nn * 4);
-  b_img_scan.ensure(nn * 4);
   if (n > 0) {
-    k_ingest_count<PT><<<grid_for(n, kT), kT, 0, s>>>(pos, n, g, b_keep.as<uint32_t>(),
+    k_ingest_count<PT><<<grid_for(n, kT), kT, 0, s>>>(boxes, nbox, n, b_keep.as<uint32_t>(),
                                                       b_nimg.as<uint32_t>());
     CMH_LAUNCHED();
   }
-  exclusive_scan_u32(b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(), n, sc + 0, scan_tmp, s);
-  exclusive_scan_u32(b_nimg.as<uint32_t>(), b_img_scan.as<uint32_t>(), n, sc + 1, scan_tmp, s);
-  CMH_CUDA(cudaMemcpyAsync(h_scal, sc, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  CMH_CUDA(cudaStreamSynchronize(s));
-  const int64_t n_kept = h_scal[0], n_img = h_scal[1];
-  const int64_t np = n_kept + n_img;
-  stats.n_out = n - n_kept;
-  stats.n_images = n_img;
-  stats.n_proc = np;
-  if (np >= (int64_t)0xffffffffll) fail(CMH_ERR_CAPACITY, "more than 2^32-2 processed particles");
-
-  // ---- keys, sort, runs ----
-  const int64_t npp = std::max<int64_t>(np, 1);
-  b_keys.ensure(npp * 8);
-  b_keys_alt.ensure(npp * 8);
-  b_vals.ensure(npp * 4);
-  b_vals_alt.ensure(npp * 4);
-  b_ppos.ensure(npp * sizeof(SPos<PT>));
-  b_spos.ensure(npp * sizeof(SPos<PT>));
-  b_run_of.ensure(npp * 4);
+  exclusive_scan_u32(b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(), n, &sc->kept_total,
+                     scan_tmp, s);
+  exclusive_scan_u32(b_nimg.as<uint32_t>(), b_img_scan.as<uint32_t>(), n, &sc->img_total,
+                     scan_tmp, s);
+  k_box_totals<<<1, 32, 0, s>>>(boxes, nbox, n, b_keep_scan.as<uint32_t>(),
+                                b_img_scan.as<uint32_t>(), sc, boxd, (uint32_t)npc);
+  CMH_LAUNCHED();
   if (n > 0) {
     k_ingest_emit<PT><<<grid_for(n, kT), kT, 0, s>>>(
-        pos, n, g, b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(), b_img_scan.as<uint32_t>(),
-        b_nimg.as<uint32_t>(), sc + 0, b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
+        boxes, nbox, n, k3all, b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(),
+        b_img_scan.as<uint32_t>(), b_nimg.as<uint32_t>(), boxd, (uint32_t)npc,
+        b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
     CMH_LAUNCHED();
   }
-  CMH_CUDA(cudaEventRecord(stage_ev[0], s));
+  mark(0);
+  // ---- sort ----
   radix_sort_u64_u32(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_keys_alt.as<uint64_t>(),
-                     b_vals_alt.as<uint32_t>(), np, key_bits, sort_tmp, scan_tmp, s);
-  CMH_CUDA(cudaEventRecord(stage_ev[1], s));
+                     b_vals_alt.as<uint32_t>(), npc, &sc->np, key_bits, sort_tmp, scan_tmp, s);
+  mark(1);
+  // ---- runs, top-cell ranges, dense maps ----
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
-  uint32_t *run_scan = flag + npp;
-  if (np > 0) {
-    k_gather_flags<PT><<<grid_for(np, kT), kT, 0, s>>>(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(),
-                                                       b_ppos.as<SPos<PT>>(), b_spos.as<SPos<PT>>(),
-                                                       flag, np);
-    CMH_LAUNCHED();
-  }
-  exclusive_scan_u32(flag, run_scan, np, sc + 2, scan_tmp, s);
-  CMH_CUDA(cudaMemcpyAsync(h_scal + 2, sc + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  CMH_CUDA(cudaStreamSynchronize(s));
-  const int64_t R = h_scal[2];
-  stats.n_cells = R;
-  const int64_t RR = std::max<int64_t>(R, 1);
-  b_run_start.ensure((RR + 1) * 4);
-  b_run_g.ensure(RR * 8);
-  if (np > 0) {
-    k_runs<<<grid_for(np, kT), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, np, g,
-                                           b_run_of.as<uint32_t>(), b_run_start.as<uint32_t>(),
-                                           b_run_g.as<uint64_t>(), sc + 2);
-    CMH_LAUNCHED();
-  }
-  // ---- top-cell ranges and dense maps ----
-  b_top_first.ensure(n_top * 4);
-  b_top_end.ensure(n_top * 4);
-  b_top_slot.ensure(n_top * 4);
+  uint32_t *run_scan = flag + npc;
+  const unsigned gp = grid_for(npc, kT);
+  k_gather_flags<PT><<<gp, kT, 0, s>>>(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(),
+                                       b_ppos.as<SPos<PT>>(), b_spos.as<SPos<PT>>(), flag, sc,
+                                       npc);
+  CMH_LAUNCHED();
+  exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s);
+  k_runs<<<gp, kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, boxes, nbox, k3all, sc,
+                           b_run_of.as<uint32_t>(), b_run_start.as<uint32_t>(),
+                           b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>());
+  CMH_LAUNCHED();
   CMH_CUDA(cudaMemsetAsync(b_top_first.p, 0, n_top * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_top_end.p, 0, n_top * 4, s));
-  const unsigned gr = grid_for(RR, kT);
-  k_top_ranges<<<gr, kT, 0, s>>>(b_run_g.as<uint64_t>(), g, sc + 2, b_top_first.as<uint32_t>(),
-                                 b_top_end.as<uint32_t>());
+  CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, s));
+  k_top_ranges<<<gp, kT, 0, s>>>(b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+                                 b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>());
   CMH_LAUNCHED();
-  b_rtmp1.ensure(RR * 4);
-  b_rtmp2.ensure(RR * 4);
-  k_dense_flags<<<gr, kT, 0, s>>>(b_run_g.as<uint64_t>(), g, sc + 2, b_top_first.as<uint32_t>(),
-                                  b_top_end.as<uint32_t>(), dense_min, b_rtmp1.as<uint32_t>());
+  k_dense_flags<<<gp, kT, 0, s>>>(b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+                                  npc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(),
+                                  dense_min, b_rtmp1.as<uint32_t>());
   CMH_LAUNCHED();
-  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), R, sc + 3, scan_tmp, s);
-  CMH_CUDA(cudaMemcpyAsync(h_scal + 3, sc + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  CMH_CUDA(cudaStreamSynchronize(s));
-  const int64_t nd = h_scal[3];
-  b_maps.ensure(std::max<int64_t>(nd, 1) * g.k3 * 4);
-  b_dense_range.ensure(std::max<int64_t>(nd, 1) * sizeof(uint2));
-  if (nd > 0) {
-    CMH_CUDA(cudaMemsetAsync(b_maps.p, 0xff, nd * g.k3 * 4, s));
-    k_dense_maps<<<gr, kT, 0, s>>>(b_run_g.as<uint64_t>(), g, sc + 2, b_top_first.as<uint32_t>(),
-                                   b_top_end.as<uint32_t>(), b_rtmp1.as<uint32_t>(),
-                                   b_rtmp2.as<uint32_t>(), dense_min, b_top_slot.as<uint32_t>(),
-                                   b_dense_range.as<uint2>(), b_maps.as<int32_t>());
-    CMH_LAUNCHED();
-  }
-  // ---- befriending ----
-  b_parent.ensure(RR * 4);
-  k_iota<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);
+  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s);
+  k_clamp_dense<<<1, 32, 0, s>>>(sc, (uint32_t)nd_cap);
   CMH_LAUNCHED();
-  CMH_CUDA(cudaEventRecord(stage_ev[2], s));
-  // dense top cells joined inside (CTA each), then a fast path for every
-  // cell, a queue of the crowded ones and a warp path for those
+  CMH_CUDA(cudaMemsetAsync(b_maps.p, 0xff, (size_t)nd_cap * k3all * 4, s));
+  k_dense_maps<<<gp, kT, 0, s>>>(b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+                                 k3all, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(),
+                                 b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), dense_min,
+                                 (uint32_t)nd_cap, b_top_slot.as<uint32_t>(),
+                                 b_dense_range.as<uint2>(), b_maps.as<int32_t>());
+  CMH_LAUNCHED();
+  k_iota<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
+  CMH_LAUNCHED();
+  mark(2);
+  // ---- befriending: dense top cells inside (CTA each), fast path, queue,
+  // warp path near then far ----
   uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
-  // sc[6] queue length, sc[7..9] work counters of the dense and warp passes
-  CMH_CUDA(cudaMemsetAsync(sc + 6, 0, 4 * sizeof(uint32_t), s));
-  const unsigned gw = grid_for(RR * 32, kT);  // one warp per queued cell
-  const size_t dsm = (size_t)g.k3 * sizeof(uint32_t);
-  const unsigned gd = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nd, (int64_t)kSMs * 16));
-#define CMH_BEFRIEND(FP)                                                                      \
-  if (nd > 0) {                                                                               \
-    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<PT, FP>,                                   \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));    \
-    k_befriend_dense<PT, FP><<<gd, 128, dsm, s>>>(g, b_run_start.as<uint32_t>(),              \
-                                                  b_run_g.as<uint64_t>(),                     \
-                                                  b_dense_range.as<uint2>(), sc + 3, sc + 7,  \
-                                                  b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), \
-                                                  b_parent.as<uint32_t>(), c);                \
-    CMH_LAUNCHED();                                                                           \
-  }                                                                                           \
-  k_befriend_simple<PT, FP><<<gr, kT, 0, s>>>(g, b_run_start.as<uint32_t>(),                 \
-                                              b_run_g.as<uint64_t>(), sc + 2,                 \
-                                              b_top_first.as<uint32_t>(),                     \
-                                              b_top_end.as<uint32_t>(), dense_min,            \
-                                              b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), \
-                                              queue, sc + 6, c);                              \
-  CMH_LAUNCHED();                                                                             \
-  k_befriend<PT, FP, 0><<<gw, kT, 0, s>>>(                                                    \
-      g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(), queue, sc + 6, sc + 8,          \
-      b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),       \
-      b_maps.as<int32_t>(), dense_min, b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);  \
-  CMH_LAUNCHED();                                                                             \
-  k_compress<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);                              \
-  CMH_LAUNCHED();                                                                             \
-  k_befriend<PT, FP, 1><<<gw, kT, 0, s>>>(                                                    \
-      g, b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(), queue, sc + 6, sc + 9,          \
-      b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),       \
-      b_maps.as<int32_t>(), dense_min, b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);  \
-  CMH_LAUNCHED()
-  if (fp32) {
-    CMH_BEFRIEND(true);
-  } else {
-    CMH_BEFRIEND(false);
-  }
-#undef CMH_BEFRIEND
-  k_compress<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), sc + 2);
+  const unsigned gw = grid_for(npc * 32, kT);
+  const size_t dsm = (size_t)k3all * sizeof(uint32_t);
+  const unsigned gd = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nd_cap, (int64_t)kSMs * 16));
+  auto befriend = [&](auto fp32_tag) {
+    constexpr bool FP = decltype(fp32_tag)::value;
+    k_befriend_dense<PT, FP><<<gd, 128, dsm, s>>>(
+        boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
+        b_run_g.as<uint64_t>(), b_dense_range.as<uint2>(), sc, (uint32_t)nd_cap,
+        b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);
+    CMH_LAUNCHED();
+    k_befriend_simple<PT, FP><<<gp, kT, 0, s>>>(
+        boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(),
+        sc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),
+        b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), queue, c);
+    CMH_LAUNCHED();
+    k_befriend<PT, FP, 0><<<gw, kT, 0, s>>>(
+        boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
+        b_run_g.as<uint64_t>(), queue, sc, b_top_first.as<uint32_t>(),
+        b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
+        b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);
+    CMH_LAUNCHED();
+    k_compress<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
+    CMH_LAUNCHED();
+    k_befriend<PT, FP, 1><<<gw, kT, 0, s>>>(
+        boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
+        b_run_g.as<uint64_t>(), queue, sc, b_top_first.as<uint32_t>(),
+        b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
+        b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);
+    CMH_LAUNCHED();
+  };
+  if (fp32) befriend(std::true_type{});
+  else befriend(std::false_type{});
+  k_compress<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
-  CMH_CUDA(cudaEventRecord(stage_ev[3], s));
+  mark(3);
 
   // ---- groups, candidates ----
-  b_count.ensure(RR * 4);
-  b_head.ensure(RR * 4);
-  b_cand_of_root.ensure(RR * 4);
-  CMH_CUDA(cudaMemsetAsync(b_count.p, 0, RR * 4, s));
-  CMH_CUDA(cudaMemsetAsync(b_head.p, 0xff, RR * 4, s));
-  CMH_CUDA(cudaMemsetAsync(b_cand_of_root.p, 0xff, RR * 4, s));
-  if (np > 0) {
-    k_group_count<<<grid_for(np, kT), kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
-                                                  b_vals.as<uint32_t>(), np, b_count.as<uint32_t>(),
-                                                  b_head.as<uint32_t>());
-    CMH_LAUNCHED();
-  }
-  k_cand_flags<<<gr, kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(), sc + 2,
-                                 g.nphalomin, b_rtmp1.as<uint32_t>(), extra + 0);
+  CMH_CUDA(cudaMemsetAsync(b_count.p, 0, npc * 4, s));
+  CMH_CUDA(cudaMemsetAsync(b_head.p, 0xff, npc * 4, s));
+  CMH_CUDA(cudaMemsetAsync(b_cand_of_root.p, 0xff, npc * 4, s));
+  k_group_count<<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
+                                  b_vals.as<uint32_t>(), sc, b_count.as<uint32_t>(),
+                                  b_head.as<uint32_t>());
   CMH_LAUNCHED();
-  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), R, sc + 4, scan_tmp, s);
-  CMH_CUDA(cudaMemcpyAsync(h_scal + 4, sc + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  CMH_CUDA(cudaStreamSynchronize(s));
-  const int64_t nc = h_scal[4];
-  const int64_t ncc = std::max<int64_t>(nc, 1);
-  b_cand_root.ensure(ncc * 4);
-  k_cand_list<<<gr, kT, 0, s>>>(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), sc + 2,
+  k_cand_flags<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(),
+                                 b_run_box.as<uint16_t>(), boxes, sc, npc,
+                                 b_rtmp1.as<uint32_t>(), extra + 0);
+  CMH_LAUNCHED();
+  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nc, scan_tmp, s);
+  k_cand_list<<<gp, kT, 0, s>>>(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), sc,
                                 b_cand_of_root.as<uint32_t>(), b_cand_root.as<uint32_t>());
   CMH_LAUNCHED();
-  CMH_CUDA(cudaEventRecord(stage_ev[4], s));
+  mark(4);
 
   // ---- property sums, ownership, catalog ----
-  const int NS = 6 + ((g.props & 1) ? 6 : 0) + ((g.props & 2) ? 6 : 0);
-  b_sums.ensure(ncc * NS * 8);
-  b_warn.ensure(ncc * 4);
-  CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, ncc * NS * 8, s));
-  CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, ncc * 4, s));
-  if (np > 0 && nc > 0) {
-    const unsigned gp = grid_for(np, kT);
-    if (NS == 6)
-      k_group_sums<PT, VT, 6><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
-                                                b_cand_of_root.as<uint32_t>(), b_spos.as<SPos<PT>>(),
-                                                vel, np, g, b_sums.as<double>(), b_warn.as<uint32_t>());
-    else if (NS == 12)
-      k_group_sums<PT, VT, 12><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
-                                                 b_cand_of_root.as<uint32_t>(), b_spos.as<SPos<PT>>(),
-                                                 vel, np, g, b_sums.as<double>(), b_warn.as<uint32_t>());
-    else
-      k_group_sums<PT, VT, 18><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
-                                                 b_cand_of_root.as<uint32_t>(), b_spos.as<SPos<PT>>(),
-                                                 vel, np, g, b_sums.as<double>(), b_warn.as<uint32_t>());
-    CMH_LAUNCHED();
-  }
-  CMH_CUDA(cudaEventRecord(stage_ev[5], s));
-  b_own.ensure(ncc * 4);
-  b_own_scan.ensure(ncc * 4);
-  const unsigned gc = grid_for(ncc, kT);
-  if (NS == 6)
-    k_owned<6><<<gc, kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),
-                                 b_count.as<uint32_t>(), sc + 4, g, b_own.as<uint32_t>());
-  else if (NS == 12)
-    k_owned<12><<<gc, kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),
-                                  b_count.as<uint32_t>(), sc + 4, g, b_own.as<uint32_t>());
-  else
-    k_owned<18><<<gc, kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),
-                                  b_count.as<uint32_t>(), sc + 4, g, b_own.as<uint32_t>());
+  const int NS = 6 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
+  CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, s));
+  CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, (size_t)ncc * 4, s));
+#define CMH_SUMS(NSV)                                                                         \
+  k_group_sums<PT, NSV><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),  \
+                                          b_cand_of_root.as<uint32_t>(),                      \
+                                          b_run_box.as<uint16_t>(), boxes,                    \
+                                          b_spos.as<SPos<PT>>(), sc, props,                   \
+                                          b_sums.as<double>(), b_warn.as<uint32_t>())
+  if (NS == 6) CMH_SUMS(6);
+  else if (NS == 12) CMH_SUMS(12);
+  else CMH_SUMS(18);
+#undef CMH_SUMS
   CMH_LAUNCHED();
-  exclusive_scan_u32(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(), nc, sc + 5, scan_tmp, s);
-  CMH_CUDA(cudaMemcpyAsync(h_scal + 5, sc + 5, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  CMH_CUDA(cudaStreamSynchronize(s));
-  const int64_t nh = h_scal[5];
-  const int64_t nhh = std::max<int64_t>(nh, 1);
-  b_okeys.ensure(nhh * 4);
-  b_ovals.ensure(nhh * 4);
-  b_okeys_alt.ensure(nhh * 4);
-  b_ovals_alt.ensure(nhh * 4);
+  mark(5);
+  const unsigned gc = grid_for(ncc, kT);
+#define CMH_OWNED(NSV)                                                                          \
+  k_owned<NSV><<<gc, kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),              \
+                                 b_count.as<uint32_t>(), b_run_box.as<uint16_t>(), boxes, sc, \
+                                 ncc, b_own.as<uint32_t>())
+  if (NS == 6) CMH_OWNED(6);
+  else if (NS == 12) CMH_OWNED(12);
+  else CMH_OWNED(18);
+#undef CMH_OWNED
+  CMH_LAUNCHED();
+  exclusive_scan_u32(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(), ncc, &sc->nh, scan_tmp, s);
   k_own_list<<<gc, kT, 0, s>>>(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(),
-                               b_cand_root.as<uint32_t>(), b_head.as<uint32_t>(), sc + 4,
+                               b_cand_root.as<uint32_t>(), b_head.as<uint32_t>(), sc,
                                b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>());
   CMH_LAUNCHED();
   radix_sort_u32_u32(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), b_okeys_alt.as<uint32_t>(),
-                     b_ovals_alt.as<uint32_t>(), nh, bits_for((uint64_t)npp), sort_tmp, scan_tmp, s);
-  b_props.ensure(nhh * g.hs * 4);
-  b_head_out.ensure(nhh * 4);
-  b_cat_of_cand.ensure(ncc * 4);
-  CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, ncc * 4, s));
-  const unsigned gh = grid_for(nhh, kT);
-#define CMH_CATALOG(NSV)                                                                    \
-  k_catalog<NSV><<<gh, kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc + 5, \
-                                   b_sums.as<double>(), b_cand_root.as<uint32_t>(),         \
-                                   b_count.as<uint32_t>(), b_warn.as<uint32_t>(), g,        \
-                                   b_props.as<float>(), b_head_out.as<uint32_t>(),          \
+                     b_ovals_alt.as<uint32_t>(), ncc, &sc->nh, bits_for((uint64_t)npc),
+                     sort_tmp, scan_tmp, s);
+  CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, (size_t)ncc * 4, s));
+#define CMH_CATALOG(NSV)                                                                        \
+  k_catalog<NSV><<<gc, kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc,          \
+                                   b_sums.as<double>(), b_cand_root.as<uint32_t>(),             \
+                                   b_count.as<uint32_t>(), b_warn.as<uint32_t>(),               \
+                                   b_run_box.as<uint16_t>(), boxd, nbox, props, hs,              \
+                                   b_props.as<float>(), b_head_out.as<uint32_t>(),              \
                                    b_cat_of_cand.as<uint32_t>(), extra + 1)
   if (NS == 6) CMH_CATALOG(6);
   else if (NS == 12) CMH_CATALOG(12);
   else CMH_CATALOG(18);
 #undef CMH_CATALOG
   CMH_LAUNCHED();
-  CMH_CUDA(cudaEventRecord(stage_ev[6], s));
+  k_halo_base<<<1, 32, 0, s>>>(boxd, nbox);
+  CMH_LAUNCHED();
+  mark(6);
+  if (want_member && n > 0) {
+    CMH_CUDA(cudaMemsetAsync(b_member.p, 0xff, (size_t)n * 8, s));
+    CMH_CUDA(cudaMemsetAsync(b_member_proc.p, 0xff, (size_t)n * 4, s));
+    CMH_CUDA(cudaMemsetAsync(b_member_pos.p, 0, (size_t)n * 12, s));
+    k_member<PT><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
+                                   b_cand_of_root.as<uint32_t>(), b_cat_of_cand.as<uint32_t>(),
+                                   b_spos.as<SPos<PT>>(), sc, b_member.as<unsigned long long>());
+    CMH_LAUNCHED();
+    k_member_copy<PT><<<gp, kT, 0, s>>>(
+        b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(), b_cand_of_root.as<uint32_t>(),
+        b_cat_of_cand.as<uint32_t>(), b_run_box.as<uint16_t>(), boxd, nbox,
+        b_spos.as<SPos<PT>>(), b_vals.as<uint32_t>(), sc, b_member.as<unsigned long long>(),
+        b_member_proc.as<uint32_t>(), b_member_pos.as<float>(), c);
+    CMH_LAUNCHED();
+  }
+  mark(7);
+}
+
+void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
+  const int nbox = (int)specs.size();
+  if (nbox < 1 || nbox > kMaxBoxes) fail(CMH_ERR_INVALID_ARGUMENT, "1 to 1024 boxes per run");
+  boxes_host.resize(nbox);
+  n_total = 0;
+  uint64_t tops = 0;
+  int kmax = 1;
+  double img = 0.0;
+  props = -1;
+  for (int b = 0; b < nbox; b++) {
+    const BoxSpec &sp = specs[b];
+    BoxDev &bd = boxes_host[b];
+    memset(&bd, 0, sizeof bd);
+    bd.g = make_geometry(sp.params, sp.ltab, sp.n, sp.cell_factor);
+    if (props < 0) props = bd.g.props;
+    if (bd.g.props != props) fail(CMH_ERR_INVALID_ARGUMENT, "boxes of a run share the property set");
+    bd.pos = sp.pos;
+    bd.vel = sp.vel;
+    bd.vel_f64 = sp.vel_f64 ? 1 : 0;
+    bd.n = (uint32_t)sp.n;
+    bd.in_base = (uint64_t)n_total;
+    bd.top_base = tops;
+    n_total += sp.n;
+    tops += (uint64_t)bd.g.T[0] * bd.g.T[1] * bd.g.T[2];
+    kmax = std::max(kmax, bd.g.k);
+    img += image_estimate(bd.g, sp.n);
+  }
+  if (n_total >= (int64_t)0xfffffff0ll) fail(CMH_ERR_CAPACITY, "more than 2^32 input particles in a run");
+  hs = 7 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
+  k3all = (uint64_t)kmax * kmax * kmax;
+  n_top = tops;
+  key_bits = bits_for(tops * k3all - 1);
+  if (tops >= (1ull << 40) || key_bits > 62) fail(CMH_ERR_CAPACITY, "too many cells in a run");
+  // capacities: grown after a run that overflowed them, never shrunk
+  const int64_t want_np = std::min<int64_t>(n_total + (int64_t)img, (int64_t)0xfffffff0ll);
+  np_cap = std::max<int64_t>(np_cap, std::max<int64_t>(want_np, 1));
+  nd_cap = std::max<int64_t>(nd_cap, np_cap / 256 + 256);
+  double mincut = 1e300;
+  for (const BoxDev &bd : boxes_host) mincut = std::min(mincut, bd.g.nphalomin);
+  const int64_t div = (int64_t)std::max(1.0, std::floor(mincut));
+  nc_cap = std::max<int64_t>(1, np_cap / div + 1);
+
+  const int64_t nn = std::max<int64_t>(n_total, 1), npc = np_cap, ncc = nc_cap;
+  scal.ensure(sizeof(DevScal));
+  ctr.ensure(sizeof(Counters) + 2 * sizeof(unsigned long long));
+  b_boxes.ensure(sizeof(BoxDev) * nbox);
+  b_boxd.ensure(sizeof(uint32_t) * 7 * nbox);
+  b_keep.ensure(nn * 4);
+  b_nimg.ensure(nn * 4);
+  b_keep_scan.ensure(nn * 4);
+  b_img_scan.ensure(nn * 4);
+  b_keys.ensure(npc * 8);
+  b_keys_alt.ensure(npc * 8);
+  b_vals.ensure(npc * 4);
+  b_vals_alt.ensure(npc * 4);
+  const size_t rec = pos_dtype == CMH_FLOAT64 ? sizeof(SPos<double>) : sizeof(SPos<float>);
+  b_ppos.ensure(npc * rec);
+  b_spos.ensure(npc * rec);
+  b_run_of.ensure(npc * 4);
+  b_run_start.ensure((npc + 1) * 4);
+  b_run_g.ensure(npc * 8);
+  b_run_box.ensure(npc * 2);
+  b_top_first.ensure(n_top * 4);
+  b_top_end.ensure(n_top * 4);
+  b_top_slot.ensure(n_top * 4);
+  b_rtmp1.ensure(npc * 4);
+  b_rtmp2.ensure(npc * 4);
+  b_maps.ensure((size_t)nd_cap * k3all * 4);
+  b_dense_range.ensure((size_t)nd_cap * sizeof(uint2));
+  b_parent.ensure(npc * 4);
+  b_count.ensure(npc * 4);
+  b_head.ensure(npc * 4);
+  b_cand_of_root.ensure(npc * 4);
+  b_cand_root.ensure(ncc * 4);
+  b_sums.ensure(ncc * 18 * 8);
+  b_warn.ensure(ncc * 4);
+  b_own.ensure(ncc * 4);
+  b_own_scan.ensure(ncc * 4);
+  b_okeys.ensure(ncc * 4);
+  b_ovals.ensure(ncc * 4);
+  b_okeys_alt.ensure(ncc * 4);
+  b_ovals_alt.ensure(ncc * 4);
+  b_props.ensure(ncc * hs * 4);
+  b_head_out.ensure(ncc * 4);
+  b_cat_of_cand.ensure(ncc * 4);
   if (want_member) {
     b_member.ensure(nn * 8);
     b_member_proc.ensure(nn * 4);
     b_member_pos.ensure(nn * 12);
-    CMH_CUDA(cudaMemsetAsync(b_member.p, 0xff, nn * 8, s));
-    CMH_CUDA(cudaMemsetAsync(b_member_proc.p, 0xff, nn * 4, s));
-    CMH_CUDA(cudaMemsetAsync(b_member_pos.p, 0, nn * 12, s));
-    if (np > 0) {
-      k_member<PT><<<grid_for(np, kT), kT, 0, s>>>(
-          b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(), b_cand_of_root.as<uint32_t>(),
-          b_cat_of_cand.as<uint32_t>(), b_spos.as<SPos<PT>>(), np,
-          b_member.as<unsigned long long>());
-      CMH_LAUNCHED();
-      k_member_copy<PT><<<grid_for(np, kT), kT, 0, s>>>(
-          b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(), b_cand_of_root.as<uint32_t>(),
-          b_cat_of_cand.as<uint32_t>(), b_spos.as<SPos<PT>>(), b_vals.as<uint32_t>(), np,
-          b_member.as<unsigned long long>(), b_member_proc.as<uint32_t>(),
-          b_member_pos.as<float>(), c);
-      CMH_LAUNCHED();
-    }
   }
-  CMH_CUDA(cudaEventRecord(ev1, s));
-  // ---- statistics ----
+  // shared memory of the dense-top kernel: one parent per fine cell of a top
+  // cell (set here, outside any graph capture)
+  {
+    const int dsm = (int)(k3all * sizeof(uint32_t));
+    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<float, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<float, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<double, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<double, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+  }
+  // pre-grow the scratch of the scans and sorts so that issue() allocates
+  // nothing (it may be captured in a graph)
+  {
+    int64_t need = 0;
+    for (int64_t m = std::max(npc, nn) * 1; m > 4096;) {
+      m = (m + 4095) / 4096;
+      need += 2 * m;
+    }
+    const int64_t ntiles = (npc + 4095) / 4096;
+    int64_t need_h = 0;
+    for (int64_t m = ntiles * 256; m > 4096;) {
+      m = (m + 4095) / 4096;
+      need_h += 2 * m;
+    }
+    scan_tmp.ensure((size_t)(std::max(need, need_h) + 16) * sizeof(uint32_t));
+    sort_tmp.ensure((size_t)(2 * ntiles * 256 + 64) * sizeof(uint32_t));
+  }
+}
+
+void Plan::read_back(cudaStream_t s, bool timed) {
+  const int nbox = (int)boxes_host.size();
   struct {
     Counters c;
     unsigned long long ngroups, nwarn;
   } hc;
+  DevScal hs_;
   CMH_CUDA(cudaMemcpyAsync(&hc, ctr.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+  CMH_CUDA(cudaMemcpyAsync(&hs_, scal.p, sizeof(DevScal), cudaMemcpyDeviceToHost, s));
+  boxd_host.resize(7 * nbox);
+  CMH_CUDA(cudaMemcpyAsync(boxd_host.data(), b_boxd.p, sizeof(uint32_t) * 7 * nbox,
+                           cudaMemcpyDeviceToHost, s));
   CMH_CUDA(cudaStreamSynchronize(s));
+  last = hs_;
   if (hc.c.uf_giveups)
     fail(CMH_ERR_DEVICE_TIMEOUT, "union-find retry loop reached its iteration cap");
-  float ms = 0;
-  CMH_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-  {
-    cudaEvent_t b[9] = {ev0, stage_ev[0], stage_ev[1], stage_ev[2], stage_ev[3],
-                        stage_ev[4], stage_ev[5], stage_ev[6], ev1};
-    for (int q = 0; q < 8; q++) CMH_CUDA(cudaEventElapsedTime(&stats.stage_ms[q], b[q], b[q + 1]));
-  }
-  stats.n_launches = (int32_t)(g_launches - launches0);
+  stats = cmh_stats{};
+  stats.n_in = n_total;
+  stats.n_out = n_total - hs_.kept_total;
+  stats.n_images = hs_.img_total;
+  stats.n_proc = hs_.np;
+  stats.n_cells = hs_.R;
   stats.n_groups = (int64_t)hc.ngroups;
-  stats.n_candidates = nc;
-  stats.nhalos = nh;
+  stats.n_candidates = hs_.nc;
+  stats.nhalos = hs_.nh;
   stats.n_edge_warn = (int64_t)hc.nwarn;
   stats.n_pair_tests = (int64_t)hc.c.pair_tests;
   stats.n_rechecks = (int64_t)hc.c.rechecks;
+  stats.n_member_conflicts = (int64_t)hc.c.member_conflicts;
+  stats.cell_factor = boxes_host[0].g.k;
+  stats.key_bits = key_bits;
   stats.n_cell_pairs = (int64_t)hc.c.cand_pairs;
   stats.n_root_skips = (int64_t)hc.c.root_skips;
   stats.n_unions = (int64_t)hc.c.unions;
   stats.n_find_steps = (int64_t)hc.c.find_steps;
   stats.n_scan_iters = (int64_t)hc.c.scan_iters;
   stats.n_window_iters = (int64_t)hc.c.window_iters;
-  stats.n_dense_tops = (int64_t)nd;
-  stats.n_member_conflicts = (int64_t)hc.c.member_conflicts;
-  stats.cell_factor = g.k;
-  stats.key_bits = key_bits;
-  stats.ms_total = ms;
-  out_nhalos = nh;
+  stats.n_dense_tops = hs_.nd;
+  if (timed) {
+    float ms = 0;
+    CMH_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    stats.ms_total = ms;
+    cudaEvent_t b[9] = {ev0, stage_ev[0], stage_ev[1], stage_ev[2], stage_ev[3],
+                        stage_ev[4], stage_ev[5], stage_ev[6], ev1};
+    for (int q = 0; q < 8; q++) CMH_CUDA(cudaEventElapsedTime(&stats.stage_ms[q], b[q], b[q + 1]));
+  }
+  out_nhalos = hs_.nh;
+}
+
+void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaStream_t s) {
+  CMH_CUDA(cudaSetDevice(device));
+  for (int attempt = 0; attempt < 3; attempt++) {
+    prepare(specs, want_member);
+    // the graph stays valid while the inputs, sizes and capacities do
+    std::vector<unsigned char> sig(sizeof(BoxDev) * boxes_host.size());
+    memcpy(sig.data(), boxes_host.data(), sig.size());
+    const int64_t caps[6] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
+                             (int64_t)dense_min};
+    sig.insert(sig.end(), (const unsigned char *)caps, (const unsigned char *)caps + sizeof caps);
+    const bool same = graph_exec && sig == graph_sig;
+    if (!same) {
+      CMH_CUDA(cudaMemcpyAsync(b_boxes.p, boxes_host.data(), sizeof(BoxDev) * boxes_host.size(),
+                               cudaMemcpyHostToDevice, s));
+      CMH_CUDA(cudaStreamSynchronize(s));
+    }
+    const long long l0 = g_launches;
+    if (use_graph && same) {
+      // a replay is timed as a whole; stage times come from eager runs
+      CMH_CUDA(cudaEventRecord(ev0, s));
+      CMH_CUDA(cudaGraphLaunch(graph_exec, s));
+      CMH_CUDA(cudaEventRecord(ev1, s));
+      launches_per_run_graph_ok = true;
+      read_back(s, false);
+      CMH_CUDA(cudaEventElapsedTime(&stats.ms_total, ev0, ev1));
+    } else {
+      if (pos_dtype == CMH_FLOAT64) issue<double>(want_member, s, true);
+      else issue<float>(want_member, s, true);
+      read_back(s, true);
+      launches_per_run = (int32_t)(g_launches - l0);
+      if (!(last.overflow & 1u) && use_graph) capture(want_member, s, sig);
+    }
+    stats.n_launches = launches_per_run;
+    if (last.overflow & 2u) nd_cap = (int64_t)last.nd + last.nd / 4 + 256;  // faster next time
+    if (!(last.overflow & 1u)) return;
+    np_cap = (int64_t)last.np_raw + last.np_raw / 8 + 4096;  // repeat with room
+  }
+  fail(CMH_ERR_CAPACITY, "processed particles kept outgrowing the buffers");
+}
+
+void Plan::capture(bool want_member, cudaStream_t s, const std::vector<unsigned char> &sig) {
+  if (graph_exec) {
+    cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+  }
+  // recorded on the plan's own stream (the legacy stream cannot be
+  // captured); the graph is then launched on the caller's stream
+  if (!cap_stream) CMH_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+  cudaGraph_t graph = nullptr;
+  CMH_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    if (pos_dtype == CMH_FLOAT64) issue<double>(want_member, cap_stream, false);
+    else issue<float>(want_member, cap_stream, false);
+  } catch (...) {
+    cudaStreamEndCapture(cap_stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  CMH_CUDA(cudaStreamEndCapture(cap_stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  CMH_CUDA(e);
+  graph_sig = sig;
+  (void)s;
 }
 
 void Plan::run(const cmh_particles &parts, bool want_member, cudaStream_t s) {
-  CMH_CUDA(cudaSetDevice(device));
-  setup_geometry(parts.n);
-  const bool pd = parts.pos_dtype == CMH_FLOAT64, vd = parts.vel_dtype == CMH_FLOAT64;
-  if (pd && vd) run_typed<double, double>(parts, want_member, s);
-  else if (pd) run_typed<double, float>(parts, want_member, s);
-  else if (vd) run_typed<float, double>(parts, want_member, s);
-  else run_typed<float, float>(parts, want_member, s);
+  BoxSpec sp;
+  sp.params = params;
+  sp.ltab = ltab_host;
+  sp.pos = parts.pos;
+  sp.vel = parts.vel;
+  sp.vel_f64 = parts.vel_dtype == CMH_FLOAT64;
+  sp.n = parts.n;
+  sp.cell_factor = 0;
+  run_batch({sp}, want_member, s);
 }
 
 }  // namespace cmh

@@ -6,6 +6,9 @@
 
 namespace cmh {
 
+constexpr int kMaxBoxes = 1024;       // domains per run
+constexpr int kMaxCellFactor = 32;    // fine cells per top-cell edge
+
 // Particle position in cell order with the index of its source particle.
 template <class PT> struct SPos;
 template <> struct __align__(16) SPos<float> {
@@ -47,6 +50,28 @@ struct Geom {
   int ltab_n;
   double ltab_dr;
   const double *ltab;    // device copy of the table
+};
+
+// One domain of a run (a run holds one or many), in device memory.
+struct BoxDev {
+  Geom g;
+  const void *pos;      // n x 3, the plan's position dtype
+  const void *vel;      // n x 3
+  uint64_t in_base;     // first index of the box in the run's input numbering
+  uint64_t top_base;    // first index of the box's top cells in the run's tables
+  uint32_t n;           // input particles of the box
+  int vel_f64;          // velocities are double
+};
+
+// Device-side sizes of one run: nothing is read back by the host until the
+// run has been issued, so the whole run can be captured in a CUDA graph.
+struct DevScal {
+  uint32_t kept_total, img_total;  // totals of the keep / image scans
+  uint32_t np_raw, np;             // processed particles (np clamped to the capacity)
+  uint32_t R, nd, nc, nh;          // fine cells, dense top cells, candidates, halos
+  uint32_t qcount, next_dense, next0, next1;
+  uint32_t overflow;               // bit 0: processed particles above capacity
+  uint32_t pad[3];
 };
 
 // Running counters of one run, in device memory.

@@ -1,4 +1,5 @@
-// A FoF plan: run parameters, device workspace and the last run's outputs.
+// A FoF plan: run parameters, device workspace, the captured graph of the
+// last run shape and the last run's outputs.
 #pragma once
 
 #include <vector>
@@ -12,42 +13,70 @@ struct cmh_plan {
 
 namespace cmh {
 
+// One domain of a run as the host describes it.
+struct BoxSpec {
+  cmh_fof_params params{};
+  std::vector<double> ltab;
+  const void *pos = nullptr;
+  const void *vel = nullptr;
+  bool vel_f64 = false;
+  int64_t n = 0;
+  int cell_factor = 0;  // 0: the params' value, or the autotuned one
+};
+
 struct Plan : public cmh_plan {
   int device = 0;
   cmh_fof_params params{};
   std::vector<double> ltab_host;
   int pos_dtype = CMH_FLOAT32;
   bool fp32 = true;
+  bool use_graph = true;    // replay the captured run when its shape repeats
   uint32_t dense_min = 16;  // top cells with more occupied fine cells get a map
 
-  Geom geom{};
-  uint64_t n_top = 0;
-  int key_bits = 0;
-  cmh_stats stats{};
-  int64_t out_nhalos = 0;
+  // shape of the current run
+  std::vector<BoxDev> boxes_host;
+  int64_t n_total = 0;
+  uint64_t n_top = 0, k3all = 1;
+  int key_bits = 0, hs = 7, props = 0;
+  int64_t np_cap = 0, nd_cap = 0, nc_cap = 0;  // grown on overflow, never shrunk
 
-  uint32_t *h_scal = nullptr;  // pinned host copy of the device scalars
+  // results of the last run
+  cmh_stats stats{};
+  DevScal last{};
+  std::vector<uint32_t> boxd_host;  // per box: 7 arrays of nbox (see k_box_totals)
+  int64_t out_nhalos = 0;
+  int32_t launches_per_run = 0;
+  bool launches_per_run_graph_ok = false;
+
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t stage_ev[7] = {};  // boundaries between the eight stages
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<unsigned char> graph_sig;
+  cudaStream_t cap_stream = nullptr;  // the stream runs are recorded on
 
   // workspace
-  DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev;
+  DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
   DevBuf b_keep, b_nimg, b_keep_scan, b_img_scan;
   DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_run_of;
-  DevBuf b_run_start, b_run_g, b_top_first, b_top_end, b_top_slot, b_rtmp1, b_rtmp2, b_maps;
+  DevBuf b_run_start, b_run_g, b_run_box, b_top_first, b_top_end, b_top_slot, b_rtmp1, b_rtmp2;
+  DevBuf b_maps, b_dense_range;
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
   DevBuf in_pos, in_vel;  // device copies of host-resident particles
-  DevBuf b_dense_range;   // first/end fine cell of each dense top cell
 
   Plan(const cmh_fof_params &p, int pos_dtype, int device);
   ~Plan() override;
   void set_params(const cmh_fof_params &p);
-  void setup_geometry(int64_t n_in);
+  Geom make_geometry(const cmh_fof_params &p, const std::vector<double> &ltab, int64_t n_in,
+                     int cell_factor) const;
+  void prepare(const std::vector<BoxSpec> &specs, bool want_member);
+  template <class PT>
+  void issue(bool want_member, cudaStream_t s, bool timed);
+  void read_back(cudaStream_t s, bool timed);
+  void capture(bool want_member, cudaStream_t s, const std::vector<unsigned char> &sig);
+  void run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaStream_t s);
   void run(const cmh_particles &parts, bool want_member, cudaStream_t s);
-  template <class PT, class VT>
-  void run_typed(const cmh_particles &parts, bool want_member, cudaStream_t s);
 };
 
 }  // namespace cmh

@@ -49,10 +49,12 @@ __device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t *warp_s
 }
 
 template <class K>
-__global__ void __launch_bounds__(kThreads) k_rs_hist(const K *__restrict__ keys, int64_t n,
+__global__ void __launch_bounds__(kThreads) k_rs_hist(const K *__restrict__ keys, int64_t n_cap,
+                                                      const uint32_t *__restrict__ n_dev,
                                                       int shift, uint32_t *__restrict__ hist,
                                                       int64_t ntiles) {
   __shared__ uint32_t h[kBins];
+  const int64_t n = n_dev ? (int64_t)*n_dev : n_cap;
   h[threadIdx.x] = 0;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kTile;
@@ -85,8 +87,10 @@ struct ScatterSmem {
 template <class K>
 __global__ void __launch_bounds__(kSThreads) k_rs_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-    K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n, int shift,
-    const uint32_t *__restrict__ hist_scan, int64_t ntiles) {
+    K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n_cap,
+    const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ hist_scan,
+    int64_t ntiles) {
+  const int64_t n = n_dev ? (int64_t)*n_dev : n_cap;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem<K> &sm = *reinterpret_cast<ScatterSmem<K> *>(smem_raw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -164,7 +168,8 @@ __global__ void __launch_bounds__(kSThreads) k_rs_scatter(
 
 template <class K>
 void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, int64_t n,
-                     int bits, DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s) {
+                     const uint32_t *n_dev, int bits, DevBuf &tmp, DevBuf &scan_tmp,
+                     cudaStream_t s) {
   if (n <= 1 || bits <= 0) return;
   const int passes = (bits + 7) / 8;
   const int64_t ntiles = (n + kTile - 1) / kTile;
@@ -175,17 +180,28 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
   uint32_t *hist = tmp.as<uint32_t>();
   uint32_t *hist_scan = hist + hn;
   const size_t smem = sizeof(ScatterSmem<K>);
-  CMH_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  {
+    // once per device, never inside a graph capture
+    static bool done[64] = {};
+    int dev = 0;
+    CMH_CUDA(cudaGetDevice(&dev));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CMH_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (dev < 64 && !done[dev] && cs == cudaStreamCaptureStatusNone) {
+      CMH_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+      done[dev] = true;
+    }
+  }
   K *src_k = keys, *dst_k = keys_alt;
   uint32_t *src_v = vals, *dst_v = vals_alt;
   for (int p = 0; p < passes; p++) {
     const int shift = 8 * p;
-    k_rs_hist<K><<<(unsigned)ntiles, kThreads, 0, s>>>(src_k, n, shift, hist, ntiles);
+    k_rs_hist<K><<<(unsigned)ntiles, kThreads, 0, s>>>(src_k, n, n_dev, shift, hist, ntiles);
     CMH_LAUNCHED();
     exclusive_scan_u32(hist, hist_scan, hn, nullptr, scan_tmp, s);
     k_rs_scatter<K><<<(unsigned)ntiles, kSThreads, smem, s>>>(src_k, src_v, dst_k, dst_v, n,
-                                                              shift, hist_scan, ntiles);
+                                                              n_dev, shift, hist_scan, ntiles);
     CMH_LAUNCHED();
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);
@@ -200,15 +216,15 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
 }  // namespace
 
 void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
-                        uint32_t *vals_alt, int64_t n, int bits, DevBuf &tmp,
-                        DevBuf &scan_tmp, cudaStream_t s) {
-  radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, bits, tmp, scan_tmp, s);
+                        uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
+                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s) {
+  radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, scan_tmp, s);
 }
 
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
-                        uint32_t *vals_alt, int64_t n, int bits, DevBuf &tmp,
-                        DevBuf &scan_tmp, cudaStream_t s) {
-  radix_sort_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, bits, tmp, scan_tmp, s);
+                        uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
+                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s) {
+  radix_sort_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, scan_tmp, s);
 }
 
 }  // namespace cmh

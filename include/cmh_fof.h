@@ -179,6 +179,17 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts,
 /* Changes the run parameters of a plan (same precision of positions). */
 cmh_status cmh_plan_set_params(cmh_plan *plan, const cmh_fof_params *params);
 
+/* A plan records the launches of a run in a CUDA graph and replays the graph
+ * when the next run has the same shape (same particle pointers and counts,
+ * parameters and capacities).  `enable` = 0 issues every run eagerly. */
+cmh_status cmh_plan_set_graph(cmh_plan *plan, int32_t enable);
+
+/* cmh_fof_run_batch on a plan: repeated batches of the same shape replay one
+ * CUDA graph. */
+cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,
+                              const cmh_particles *parts, int32_t nbox, cmh_catalog *cats,
+                              void *stream);
+
 void cmh_plan_destroy(cmh_plan *plan);
 
 /* ---- batched boxes: many independent domains in one launch sequence ----- */

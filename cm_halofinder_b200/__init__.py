@@ -222,24 +222,42 @@ class Plan:
         """Replay runs of a repeated shape from a captured CUDA graph."""
         _abi.check(self._L.cmh_plan_set_graph(self._h, int(bool(enable))))
 
-    def run_batch(self, configs, positions, velocities, stream=None):
-        """Many independent boxes in one run (one sort, one befriending pass,
-        one reduction for all of them); positions/velocities are torch CUDA
-        tensors.  Returns one host Catalog per box."""
+    def _batch_args(self, configs, positions, velocities):
         nb = len(configs)
-        P = (_abi.FofParams * nb)(*[c.to_c() for c in configs])
-        keep = [P]
+        cs = [c.to_c() for c in configs]     # keep the varlink tables alive
+        P = (_abi.FofParams * nb)(*cs)
         parts = (_abi.Particles * nb)()
         for b in range(nb):
             pos, vel = positions[b], velocities[b]
             parts[b] = _abi.Particles(n=int(pos.shape[0]), pos_dtype=self._tdt(pos),
                                       vel_dtype=self._tdt(vel), pos=self._ptr(pos),
                                       vel=self._ptr(vel), id=None, location=CMH_DEVICE)
+        return nb, P, parts, cs
+
+    @staticmethod
+    def _stream(stream):
+        if stream is None:
+            return 0
+        return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+    def autotune(self, configs, positions, velocities, repeats=2, stream=None):
+        """Time the boxes over a grid of cell-size scales and dense-map
+        thresholds; the plan keeps the fastest.  Returns the choice."""
+        nb, P, parts, _keep = self._batch_args(configs, positions, velocities)
+        t = _abi.Tuning()
+        _abi.check(self._L.cmh_plan_autotune(self._h, P, parts, nb, int(repeats),
+                                             C.c_void_p(self._stream(stream)), C.byref(t)))
+        return {"cell_scale": t.cell_scale, "dense_min": t.dense_min, "ms": t.ms,
+                "tried": t.tried}
+
+    def run_batch(self, configs, positions, velocities, stream=None):
+        """Many independent boxes in one run (one sort, one befriending pass,
+        one reduction for all of them); positions/velocities are torch CUDA
+        tensors.  Returns one host Catalog per box."""
+        nb, P, parts, _keep = self._batch_args(configs, positions, velocities)
         cats = (_abi.Catalog * nb)()
-        sp = 0 if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream")
-                                        else int(stream))
-        _abi.check(self._L.cmh_plan_run_batch(self._h, P, parts, nb, cats, C.c_void_p(sp)))
-        del keep
+        _abi.check(self._L.cmh_plan_run_batch(self._h, P, parts, nb, cats,
+                                              C.c_void_p(self._stream(stream))))
         out = []
         for b in range(nb):
             try:

@@ -73,6 +73,11 @@ class Catalog(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("cell_scale", C.c_double), ("dense_min", C.c_int32), ("ms", C.c_float),
+                ("tried", C.c_int32)]
+
+
 class RunParameters(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("Nx", "Ny", "Nz", "Px", "Py", "Pz")] + [
         (k, C.c_double) for k in ("Lxmin", "Lymin", "Lzmin", "Lxmax", "Lymax", "Lzmax")] + [
@@ -100,6 +105,8 @@ SIGNATURES = {
     "cmh_plan_set_params": (C.c_int, [C.c_void_p, C.POINTER(FofParams)]),
     "cmh_plan_destroy": (None, [C.c_void_p]),
     "cmh_plan_set_graph": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cmh_plan_autotune": (C.c_int, [C.c_void_p, C.POINTER(FofParams), C.POINTER(Particles),
+                                    C.c_int32, C.c_int32, C.c_void_p, C.POINTER(Tuning)]),
     "cmh_plan_run_batch": (C.c_int, [C.c_void_p, C.POINTER(FofParams), C.POINTER(Particles),
                                      C.c_int32, C.POINTER(Catalog), C.c_void_p]),
     "cmh_fof_run_batch": (C.c_int, [C.POINTER(FofParams), C.POINTER(Particles), C.c_int32,

@@ -326,8 +326,8 @@ cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
 }
 
 namespace {
-void run_batch_on(Plan &pl, const cmh_fof_params *params, const cmh_particles *parts,
-                  int32_t nbox, cmh_catalog *cats, cudaStream_t s) {
+std::vector<cmh::BoxSpec> make_specs(Plan &pl, const cmh_fof_params *params,
+                                     const cmh_particles *parts, int32_t nbox) {
   std::vector<cmh::BoxSpec> specs(nbox);
   for (int b = 0; b < nbox; b++) {
     check_parts(&parts[b]);
@@ -351,10 +351,28 @@ void run_batch_on(Plan &pl, const cmh_fof_params *params, const cmh_particles *p
     sp.n = parts[b].n;
   }
   pl.fp32 = params[0].precision == CMH_FP32_RECHECK;
-  pl.run_batch(specs, false, s);
+  return specs;
+}
+
+void run_batch_on(Plan &pl, const cmh_fof_params *params, const cmh_particles *parts,
+                  int32_t nbox, cmh_catalog *cats, cudaStream_t s) {
+  pl.run_batch(make_specs(pl, params, parts, nbox), false, s);
   for (int b = 0; b < nbox; b++) catalog_to_host(pl, &cats[b], false, b, s);
 }
 }  // namespace
+
+cmh_status cmh_plan_autotune(cmh_plan *plan, const cmh_fof_params *params,
+                             const cmh_particles *parts, int32_t nbox, int32_t repeats,
+                             void *stream, cmh_tuning *out) {
+  CMH_API_BEGIN
+  if (!plan || !params || !parts || nbox < 1)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan, params and particles are required");
+  Plan &pl = *static_cast<Plan *>(plan);
+  cmh_tuning t = pl.autotune(make_specs(pl, params, parts, nbox), repeats,
+                             static_cast<cudaStream_t>(stream));
+  if (out) *out = t;
+  CMH_API_END
+}
 
 cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *parts,
                              int32_t nbox, cmh_catalog *cats, void *stream) {

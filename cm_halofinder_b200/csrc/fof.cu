@@ -1231,9 +1231,10 @@ Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &lta
   }
   int k = cell_factor > 0 ? cell_factor : p.cell_factor;
   if (k <= 0) {
-    // one top cell per particle on average, as the reference's lcell = L/Px
+    // one top cell per particle on average, as the reference's lcell = L/Px,
+    // times the autotuned scale
     const double sep = std::cbrt(vol / std::max<double>((double)n_in, 1.0));
-    k = (int)std::lround(sep / g.h);
+    k = (int)std::lround(sep / g.h * cell_scale);
   }
   k = std::min(std::max(k, g.W), kMaxCellFactor);
   while (true) {
@@ -1702,6 +1703,39 @@ void Plan::capture(bool want_member, cudaStream_t s, const std::vector<unsigned 
   CMH_CUDA(e);
   graph_sig = sig;
   (void)s;
+}
+
+// Grid search over the cell-size scale and the dense-map threshold, timing
+// eager runs of the real boxes (after one untimed run per setting, which
+// also grows the buffers).  The fastest setting stays in the plan.
+cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaStream_t s) {
+  const double scales[] = {0.5, 0.75, 1.0, 1.5, 2.0};
+  const uint32_t mins[] = {8, 16, 32};
+  const bool graph0 = use_graph;
+  use_graph = false;
+  cmh_tuning best{cell_scale, (int32_t)dense_min, 1e30f, 0};
+  for (double sc : scales)
+    for (uint32_t dm : mins) {
+      cell_scale = sc;
+      dense_min = dm;
+      run_batch(specs, false, s);
+      float t = 0;
+      for (int r = 0; r < std::max(repeats, 1); r++) {
+        run_batch(specs, false, s);
+        t += stats.ms_total;
+      }
+      t /= std::max(repeats, 1);
+      best.tried++;
+      if (t < best.ms) {
+        best.ms = t;
+        best.cell_scale = sc;
+        best.dense_min = (int32_t)dm;
+      }
+    }
+  cell_scale = best.cell_scale;
+  dense_min = (uint32_t)best.dense_min;
+  use_graph = graph0;
+  return best;
 }
 
 void Plan::run(const cmh_particles &parts, bool want_member, cudaStream_t s) {

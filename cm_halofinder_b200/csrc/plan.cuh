@@ -32,6 +32,7 @@ struct Plan : public cmh_plan {
   bool fp32 = true;
   bool use_graph = true;    // replay the captured run when its shape repeats
   uint32_t dense_min = 16;  // top cells with more occupied fine cells get a map
+  double cell_scale = 1.0;  // autotuned scale of the default cell-size factor
 
   // shape of the current run
   std::vector<BoxDev> boxes_host;
@@ -76,6 +77,7 @@ struct Plan : public cmh_plan {
   void read_back(cudaStream_t s, bool timed);
   void capture(bool want_member, cudaStream_t s, const std::vector<unsigned char> &sig);
   void run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaStream_t s);
+  cmh_tuning autotune(const std::vector<BoxSpec> &specs, int repeats, cudaStream_t s);
   void run(const cmh_particles &parts, bool want_member, cudaStream_t s);
 };
 

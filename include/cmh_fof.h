@@ -184,6 +184,22 @@ cmh_status cmh_plan_set_params(cmh_plan *plan, const cmh_fof_params *params);
  * parameters and capacities).  `enable` = 0 issues every run eagerly. */
 cmh_status cmh_plan_set_graph(cmh_plan *plan, int32_t enable);
 
+/* Autotuner: times runs of these boxes (device-resident, as for
+ * cmh_plan_run_batch) over a grid of cell-size scales (fine cells per
+ * top-cell edge relative to one particle per top cell) and dense-map
+ * thresholds, `repeats` timed runs each, and keeps the fastest setting in
+ * the plan for its later runs.  Boxes whose params set cell_factor keep it. */
+typedef struct cmh_tuning {
+  double cell_scale;   /* chosen scale of the cell-size factor            */
+  int32_t dense_min;   /* chosen occupied-fine-cell threshold for a map   */
+  float ms;            /* best run time (CUDA events)                     */
+  int32_t tried;       /* settings timed                                  */
+} cmh_tuning;
+
+cmh_status cmh_plan_autotune(cmh_plan *plan, const cmh_fof_params *params,
+                             const cmh_particles *parts, int32_t nbox, int32_t repeats,
+                             void *stream, cmh_tuning *out);
+
 /* cmh_fof_run_batch on a plan: repeated batches of the same shape replay one
  * CUDA graph. */
 cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,
@@ -197,7 +213,9 @@ void cmh_plan_destroy(cmh_plan *plan);
 /* Runs `nbox` independent domains; box b uses params[b] and parts[b]
  * (device-resident, same dtypes for all boxes).  The boxes' particles are
  * processed together: one sort, one befriending pass and one reduction for
- * the whole batch.  cats[b] receives box b's catalog (host arrays). */
+ * the whole batch.  cats[b] receives box b's catalog (host arrays); its
+ * stats n_in, n_out, n_images, n_proc and nhalos are box b's, the other
+ * stats (cells, pair tests, stage times, launches) cover the whole run. */
 cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *parts,
                              int32_t nbox, cmh_catalog *cats, void *stream);
 

@@ -39,6 +39,9 @@ def build():
 
 def write_params(path, *, lo, hi, boundary, linklength, nphalomin, cells,
                  n_proc, base_in, base_out):
+    lo = [float(x) for x in lo]   # plain floats: repr of a numpy scalar is not a number
+    hi = [float(x) for x in hi]
+    boundary, linklength, nphalomin = float(boundary), float(linklength), float(nphalomin)
     ext = [hi[a] - lo[a] for a in range(3)]
     # Set_Params sizes P[] as Buffer*(1+extra)*Px*Py*Pz (startup.c:96-104);
     # pick Buffer so that the whole processing array fits.

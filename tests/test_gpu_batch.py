@@ -70,3 +70,34 @@ def test_image_overflow_reruns_with_room():
     ref = cpu.run(w)
     assert cat.stats["n_images"] == ref["stats"]["n_images"] == 7 * 20000
     assert_same_catalog(cat, ref)
+
+
+def test_autotune_keeps_results():
+    """The autotuner only changes cell sizes and the dense-map threshold; the
+    catalogs after tuning match the oracle box by box."""
+    import torch
+    boxes = _boxes(5, 9)
+    cfgs = [FofConfig.from_workload(w) for w in boxes]
+    pos = [torch.from_numpy(w.pos).cuda() for w in boxes]
+    vel = [torch.from_numpy(w.vel).cuda() for w in boxes]
+    plan = Plan(cfgs[0])
+    t = plan.autotune(cfgs, pos, vel, repeats=1)
+    assert t["tried"] == 15 and t["ms"] > 0
+    assert t["cell_scale"] in (0.5, 0.75, 1.0, 1.5, 2.0) and t["dense_min"] in (8, 16, 32)
+    cats = plan.run_batch(cfgs, pos, vel)
+    for w, cat in zip(boxes, cats):
+        assert_same_catalog(cat, cpu.run(w), check_member=False)
+
+
+@pytest.mark.parametrize("scale", [0.5, 2.0])
+def test_cell_scale_extremes(scale):
+    """The coarsest and finest cell grids the tuner tries give the same
+    catalog (set here through an explicit cell-size factor)."""
+    w = synth.config2(seed=311, scale=30000 / 256 ** 3)
+    ref = cpu.run(w)
+    sep = (float(np.prod(np.array(w.hi) - np.array(w.lo))) / w.n) ** (1 / 3)
+    h = w.linklength * (1 - 2 ** -20) / 3 ** 0.5
+    k = max(2, min(32, int(round(sep / h * scale))))
+    cat = fof(w.pos, w.vel, FofConfig.from_workload(w, cell_factor=k), members=True)
+    assert cat.stats["cell_factor"] == k
+    assert_same_catalog(cat, ref)

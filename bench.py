@@ -101,9 +101,23 @@ def make_workload(args, rank):
         return synth.config2(seed=2 + rank, scale=args.scale)
     if args.config == "c1":
         return synth.config1(seed=1 + rank, scale=args.scale)
+    if args.config == "c3":
+        return synth.config3(seed=3 + rank, scale=args.scale)
     if args.config == "c5":
         return synth.config5(seed=5 + rank, scale=args.scale)
     raise SystemExit(f"unknown config {args.config}")
+
+
+def describe(args, w):
+    dt = "FP32" if w.pos.dtype == np.float32 else "FP64"
+    if getattr(w, "varlink", None):
+        tab = w.varlink["table"]
+        return (f"{args.config}: lightcone, sphere of radius {w.hi[0]:.1f} Mpc/h around the "
+                f"observer, N={w.n}, {dt} positions, {w.meta['n_clumps']} clumps, mean density "
+                f"falling 3x outwards, l(r) from {tab.min():.4f} to {tab.max():.4f} on a "
+                f"{w.cells}^3 grid, non-periodic, Boundarysize={w.boundary}")
+    return (f"{args.config}: periodic box L={w.hi[0]:.1f} Mpc/h, N={w.n}, {dt} positions, "
+            f"{w.meta['n_clumps']} clumps, l={w.linklength:.6f}, Boundarysize={w.boundary}")
 
 
 def stage_bytes(st, pos_bytes):
@@ -254,9 +268,7 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64-recheck" if args.precision == "fp32" else "f64",
         "data": "synthetic (seeded Plummer clumps + uniform background)",
-        "config": {"workload": f"{args.config}: periodic box L={w.hi[0]:.1f} Mpc/h, "
-                               f"N={n}, FP32 positions, {w.meta['n_clumps']} clumps, "
-                               f"l={w.linklength:.6f}, Boundarysize={w.boundary}",
+        "config": {"workload": describe(args, w),
                    "n_particles": n, "n_processed": st["n_proc"], "n_images": st["n_images"],
                    "n_halos": st["nhalos"], "n_groups": st["n_groups"],
                    "n_fine_cells": st["n_cells"], "cell_factor": st["cell_factor"],
@@ -266,7 +278,8 @@ def run_ours(args):
                    "scan_iters": st["n_scan_iters"], "window_iters": st["n_window_iters"],
                    "dense_tops": st["n_dense_tops"],
                    "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "inputs (400 MB) larger than L2; no flush"},
+                   "l2": f"inputs ({(w.pos.nbytes + w.vel.nbytes) / 1e6:.0f} MB) larger than "
+                         "L2; no flush"},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "stage_ms_note": "per-stage CUDA-event times of one eager step after the timed graph replays",
         "plain_fp64": plain,

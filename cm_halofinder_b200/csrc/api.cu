@@ -67,7 +67,7 @@ Plan::~Plan() {
   if (cap_stream) cudaStreamDestroy(cap_stream);
   DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd, &b_keep,
                    &b_nimg, &b_keep_scan, &b_img_scan, &b_keys, &b_keys_alt, &b_vals,
-                   &b_vals_alt, &b_ppos, &b_spos, &b_run_of, &b_run_start, &b_run_g,
+                   &b_vals_alt, &b_ppos, &b_spos, &b_svl, &b_run_of, &b_run_start, &b_run_g,
                    &b_run_box, &b_top_first, &b_top_end, &b_top_slot, &b_rtmp1, &b_rtmp2,
                    &b_maps, &b_dense_range, &b_parent, &b_count, &b_head, &b_cand_of_root,
                    &b_cand_root, &b_sums, &b_warn, &b_own, &b_own_scan, &b_okeys, &b_ovals,

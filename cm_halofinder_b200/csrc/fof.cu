@@ -303,6 +303,41 @@ __global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ keys,
   }
 }
 
+// Grid cell and linking length of every processed particle (variable
+// linking length runs only; boxes with a fixed length get cell 0 and their
+// own l^2 / band, which reproduces the fixed-length test).
+template <class PT, bool FP32>
+__global__ void __launch_bounds__(kT) k_varlink_recs(const SPos<PT> *__restrict__ spos,
+                                                     const uint32_t *__restrict__ run_of,
+                                                     const uint16_t *__restrict__ run_box,
+                                                     const BoxDev *__restrict__ boxes,
+                                                     const DevScal *__restrict__ sc,
+                                                     VLRec<FP32> *__restrict__ svl) {
+  const int64_t np = sc->np;
+  for (int64_t i = gtid(); i < np; i += gstride()) {
+    const Geom &g = boxes[run_box[run_of[i]]].g;
+    VLRec<FP32> v;
+    double lsq = g.linksq;
+    v.rkey = 0;
+    if (g.varlink) {
+      const SPos<PT> p = spos[i];
+      v.rkey = ref_key(g, (double)p.x, (double)p.y, (double)p.z);
+      lsq = ref_cell_linksq(g, v.rkey);
+    }
+    if constexpr (FP32) {
+      if (g.varlink) {
+        band_thresholds(lsq, sizeof(PT) == 4 ? 4 : 8, &v.t_lo, &v.t_hi);
+      } else {
+        v.t_lo = g.t_lo;
+        v.t_hi = g.t_hi;
+      }
+    } else {
+      v.lsq = lsq;
+    }
+    svl[i] = v;
+  }
+}
+
 __device__ __forceinline__ uint64_t top_of_run(const BoxDev &bx, uint64_t pg) {
   const Geom &g = bx.g;
   const int k = g.k;
@@ -395,16 +430,34 @@ __global__ void __launch_bounds__(kT) k_iota(uint32_t *__restrict__ a,
 // ---------------------------------------------------------------------------
 
 // The reference's pair predicate (FOF.c:351-357), FP64 or FP32 + band recheck.
-template <class PT, bool FP32>
+// With VL (variable linking length) the pair's l^2 or band comes from the
+// lower of the two particles' grid cells, and particles of cells that are
+// not neighbours are never linked; va/vb are ignored otherwise.
+template <class PT, bool FP32, bool VL>
 __device__ __forceinline__ bool linked(const SPos<PT> &p, const SPos<PT> &q, const Geom &g,
+                                       const VLRec<FP32> &va, const VLRec<FP32> &vb,
                                        unsigned long long &rechecks) {
+  float t_lo = g.t_lo, t_hi = g.t_hi;
+  double lsq = g.linksq;
+  uint64_t rk = 0;
+  if constexpr (VL) {
+    if (!ref_neighbours(va.rkey, vb.rkey)) return false;
+    const VLRec<FP32> &v = va.rkey <= vb.rkey ? va : vb;
+    rk = v.rkey;
+    if constexpr (FP32) {
+      t_lo = v.t_lo;
+      t_hi = v.t_hi;
+    } else {
+      lsq = v.lsq;
+    }
+  }
   double dx, dy, dz;
   if constexpr (sizeof(PT) == 4) {
     const float fx = __fsub_rn(p.x, q.x), fy = __fsub_rn(p.y, q.y), fz = __fsub_rn(p.z, q.z);
     if constexpr (FP32) {
       const float d2 = __fmaf_rn(fz, fz, __fmaf_rn(fy, fy, __fmul_rn(fx, fx)));
-      if (d2 < g.t_lo) return true;
-      if (d2 > g.t_hi) return false;
+      if (d2 < t_lo) return true;
+      if (d2 > t_hi) return false;
       rechecks++;
     }
     dx = (double)fx;
@@ -418,13 +471,14 @@ __device__ __forceinline__ bool linked(const SPos<PT> &p, const SPos<PT> &q, con
       const float fx = __double2float_rn(dx), fy = __double2float_rn(dy),
                   fz = __double2float_rn(dz);
       const float d2 = __fmaf_rn(fz, fz, __fmaf_rn(fy, fy, __fmul_rn(fx, fx)));
-      if (d2 < g.t_lo) return true;
-      if (d2 > g.t_hi) return false;
+      if (d2 < t_lo) return true;
+      if (d2 > t_hi) return false;
       rechecks++;
     }
   }
+  if constexpr (VL && FP32) lsq = g.varlink ? ref_cell_linksq(g, rk) : g.linksq;
   const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-  return !(d2 > g.linksq);
+  return !(d2 > lsq);
 }
 
 // Squared distance from a point to the box of fine cell (cx, cy, cz).
@@ -475,20 +529,25 @@ struct BfStats {
 // particles of a, `apart()` is asked whether a and b are still in different
 // components (another thread may have joined them meanwhile); if not, the
 // search stops and reports no link, which is then harmless.
-template <class PT, bool FP32, class Apart>
+template <class PT, bool FP32, bool VL, class Apart>
 __device__ __forceinline__ bool cells_linked(const Geom &g, uint32_t b, int bx, int by, int bz,
                                              uint32_t sa, uint32_t ea,
                                              const uint32_t *__restrict__ run_start,
-                                             const SPos<PT> *__restrict__ spos, BfStats &st,
+                                             const SPos<PT> *__restrict__ spos,
+                                             const VLRec<FP32> *__restrict__ svl, BfStats &st,
                                              Apart apart) {
   const uint32_t sb = __ldg(run_start + b), eb = __ldg(run_start + b + 1);
   for (uint32_t i = sa; i < ea; i++) {
     if (((i - sa) & 15) == 15 && !apart()) return false;
     const SPos<PT> p = spos[i];
     if (box_dist2(g, (double)p.x, (double)p.y, (double)p.z, bx, by, bz) > g.prune_sq) continue;
+    VLRec<FP32> va{};
+    if constexpr (VL) va = svl[i];
     for (uint32_t j = sb; j < eb; j++) {
       st.tests++;
-      if (linked<PT, FP32>(p, spos[j], g, st.rechecks)) return true;
+      VLRec<FP32> vb{};
+      if constexpr (VL) vb = svl[j];
+      if (linked<PT, FP32, VL>(p, spos[j], g, va, vb, st.rechecks)) return true;
     }
   }
   return false;
@@ -499,11 +558,12 @@ __device__ __forceinline__ bool cells_linked(const Geom &g, uint32_t b, int bx, 
 // `ra` caches a root of a's component: it may be stale (a root that was hooked
 // since), but it stays in a's component, so "b reaches ra" still proves that
 // a and b are already joined.
-template <class PT, bool FP32>
+template <class PT, bool FP32, bool VL>
 __device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra, uint32_t b,
                                          int bx, int by, int bz, uint32_t sa, uint32_t ea,
                                          const uint32_t *__restrict__ run_start,
-                                         const SPos<PT> *__restrict__ spos, uint32_t *parent,
+                                         const SPos<PT> *__restrict__ spos,
+                                         const VLRec<FP32> *__restrict__ svl, uint32_t *parent,
                                          Counters *ctr, BfStats &st) {
   st.cand++;
   const uint32_t pb = __ldcg(parent + b);
@@ -516,7 +576,7 @@ __device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra
   auto apart = [&]() {
     return uf_find_n(parent, a, st.steps) != uf_find_n(parent, b, st.steps);
   };
-  if (cells_linked<PT, FP32>(g, b, bx, by, bz, sa, ea, run_start, spos, st, apart)) {
+  if (cells_linked<PT, FP32, VL>(g, b, bx, by, bz, sa, ea, run_start, spos, svl, st, apart)) {
     uf_union(parent, ra, rb, ctr);
     st.unions++;
     ra = uf_find_n(parent, ra, st.steps);
@@ -559,13 +619,13 @@ __device__ __forceinline__ void lunion(uint32_t *lp, uint32_t a, uint32_t b, Cou
 // global parent is set to its local root.  Links that cross the top cell's
 // faces are left to the global passes.  CTAs take top cells from an atomic
 // counter: their sizes differ widely.
-template <class PT, bool FP32>
+template <class PT, bool FP32, bool VL>
 __global__ void __launch_bounds__(128) k_befriend_dense(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint2 *__restrict__ dense_range, DevScal *sc, uint32_t nd_cap,
-    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos, uint32_t *parent,
-    Counters *ctr) {
+    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
+    const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr) {
   extern __shared__ uint32_t lpar[];
   __shared__ uint32_t s_slot;
   const uint32_t nd = min(sc->nd, nd_cap);
@@ -608,8 +668,8 @@ __global__ void __launch_bounds__(128) k_befriend_dense(
                 continue;
               }
               auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
-              if (cells_linked<PT, FP32>(g, (uint32_t)r, gx + dx, gy + dy, gz + dz, sa, ea,
-                                         run_start, spos, st, apart)) {
+              if (cells_linked<PT, FP32, VL>(g, (uint32_t)r, gx + dx, gy + dy, gz + dz, sa,
+                                             ea, run_start, spos, svl, st, apart)) {
                 lunion(lpar, ri, rj, ctr);
                 st.unions++;
               }
@@ -640,13 +700,14 @@ __device__ __forceinline__ bool reaches(int s, int o, int k, int W) {
 // the warp path below.
 constexpr uint32_t kSimple = 2;
 
-template <class PT, bool FP32>
+template <class PT, bool FP32, bool VL>
 __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g, DevScal *sc,
     const uint32_t *__restrict__ top_first, const uint32_t *__restrict__ top_end,
-    const uint32_t *__restrict__ top_slot, const SPos<PT> *__restrict__ spos, uint32_t *parent,
-    uint32_t *__restrict__ queue, Counters *ctr) {
+    const uint32_t *__restrict__ top_slot, const SPos<PT> *__restrict__ spos,
+    const VLRec<FP32> *__restrict__ svl, uint32_t *parent, uint32_t *__restrict__ queue,
+    Counters *ctr) {
   const uint32_t R = sc->R;
   const int lane = threadIdx.x & 31;
   BfStats st;
@@ -703,8 +764,8 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
           sa = run_start[a];
           ea = run_start[a + 1];
         }
-        try_link<PT, FP32>(g, a, ra, R0[nb] + q, bx2, by2, bz2, sa, ea, run_start, spos, parent,
-                           ctr, st);
+        try_link<PT, FP32, VL>(g, a, ra, R0[nb] + q, bx2, by2, bz2, sa, ea, run_start, spos, svl,
+                               parent, ctr, st);
       }
     }
   }
@@ -720,14 +781,14 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
 // candidates within one fine cell, PHASE 1 the farther ones, so that a dense
 // neighbourhood is joined (and compressed) before its far pairs are tried and
 // most of those become root skips.
-template <class PT, bool FP32, int PHASE>
+template <class PT, bool FP32, bool VL, int PHASE>
 __global__ void __launch_bounds__(kT) k_befriend(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint32_t *__restrict__ queue, DevScal *sc, const uint32_t *__restrict__ top_first,
     const uint32_t *__restrict__ top_end, const uint32_t *__restrict__ top_slot,
-    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos, uint32_t *parent,
-    Counters *ctr) {
+    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
+    const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr) {
   const uint32_t NQ = sc->qcount;
   uint32_t *next = PHASE == 0 ? &sc->next0 : &sc->next1;
   const int lane = threadIdx.x & 31;
@@ -833,7 +894,8 @@ __global__ void __launch_bounds__(kT) k_befriend(
       }
       const int cheb = max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz)));
       if ((PHASE == 0 && cheb > 1) || (PHASE == 1 && cheb <= 1)) continue;
-      try_link<PT, FP32>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, parent, ctr, st);
+      try_link<PT, FP32, VL>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent, ctr,
+                             st);
     }
   }
   st.flush(ctr);
@@ -1223,6 +1285,24 @@ Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &lta
   g.h = minlink * (1.0 - 0x1p-20) / std::sqrt(3.0);
   g.inv_h = 1.0 / g.h;
   g.W = (int)std::floor(maxlink / g.h * (1.0 + 1e-6)) + 1;
+  if (p.varlink) {
+    // the fixed grid of the l(r) rule (FOF.c:50-52, 63-65)
+    g.varlink = 1;
+    for (int a = 0; a < 3; a++) {
+      if (p.ref_cells[a] < 1) fail(CMH_ERR_INVALID_ARGUMENT, "ref_cells must be positive");
+      g.origin[a] = p.origin[a];
+      g.ref_lcell[a] = (p.hi[a] - p.lo[a] + 2.0 * p.boundary) / p.ref_cells[a];
+      g.ref_nc[a] = (int)std::ceil((g.rmax[a] - g.rmin[a]) / g.ref_lcell[a]) + 1;
+      if (g.ref_nc[a] >= (1 << 21)) fail(CMH_ERR_CAPACITY, "more than 2^21 grid cells along an axis");
+      // the reference scans only neighbouring cells: a longer link would be missed
+      if (maxlink > g.ref_lcell[a])
+        fail(CMH_ERR_INVALID_ARGUMENT, "linking length longer than the grid cell (raise Px/Py/Pz cells)");
+    }
+    if (ltab.size() < 2 || !(p.ltab_rmax > 0))
+      fail(CMH_ERR_INVALID_ARGUMENT, "variable linking length needs a table of 2+ values");
+    g.ltab_n = (int)ltab.size();
+    g.ltab_dr = p.ltab_rmax / (double)(g.ltab_n - 1);
+  }
   double vol = 1.0;
   for (int a = 0; a < 3; a++) {
     g.G[a] = (int)std::floor((g.rmax[a] - g.rmin[a]) / g.h) + 2;
@@ -1320,6 +1400,17 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                            b_run_of.as<uint32_t>(), b_run_start.as<uint32_t>(),
                            b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>());
   CMH_LAUNCHED();
+  if (varlink) {
+    if (fp32)
+      k_varlink_recs<PT, true><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), b_run_of.as<uint32_t>(),
+                                                 b_run_box.as<uint16_t>(), boxes, sc,
+                                                 b_svl.as<VLRec32>());
+    else
+      k_varlink_recs<PT, false><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), b_run_of.as<uint32_t>(),
+                                                  b_run_box.as<uint16_t>(), boxes, sc,
+                                                  b_svl.as<VLRec64>());
+    CMH_LAUNCHED();
+  }
   CMH_CUDA(cudaMemsetAsync(b_top_first.p, 0, n_top * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_top_end.p, 0, n_top * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, s));
@@ -1349,35 +1440,39 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   const unsigned gw = grid_for(npc * 32, kT);
   const size_t dsm = (size_t)k3all * sizeof(uint32_t);
   const unsigned gd = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nd_cap, (int64_t)kSMs * 16));
-  auto befriend = [&](auto fp32_tag) {
+  auto befriend = [&](auto fp32_tag, auto vl_tag) {
     constexpr bool FP = decltype(fp32_tag)::value;
-    k_befriend_dense<PT, FP><<<gd, 128, dsm, s>>>(
+    constexpr bool VL = decltype(vl_tag)::value;
+    const VLRec<FP> *svl = VL ? b_svl.as<VLRec<FP>>() : nullptr;
+    k_befriend_dense<PT, FP, VL><<<gd, 128, dsm, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         b_run_g.as<uint64_t>(), b_dense_range.as<uint2>(), sc, (uint32_t)nd_cap,
-        b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);
+        b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
-    k_befriend_simple<PT, FP><<<gp, kT, 0, s>>>(
+    k_befriend_simple<PT, FP, VL><<<gp, kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(),
         sc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),
-        b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), queue, c);
+        b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), queue, c);
     CMH_LAUNCHED();
-    k_befriend<PT, FP, 0><<<gw, kT, 0, s>>>(
+    k_befriend<PT, FP, VL, 0><<<gw, kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         b_run_g.as<uint64_t>(), queue, sc, b_top_first.as<uint32_t>(),
         b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
-        b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);
+        b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
     k_compress<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
     CMH_LAUNCHED();
-    k_befriend<PT, FP, 1><<<gw, kT, 0, s>>>(
+    k_befriend<PT, FP, VL, 1><<<gw, kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         b_run_g.as<uint64_t>(), queue, sc, b_top_first.as<uint32_t>(),
         b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
-        b_spos.as<SPos<PT>>(), b_parent.as<uint32_t>(), c);
+        b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
   };
-  if (fp32) befriend(std::true_type{});
-  else befriend(std::false_type{});
+  if (fp32 && varlink) befriend(std::true_type{}, std::true_type{});
+  else if (fp32) befriend(std::true_type{}, std::false_type{});
+  else if (varlink) befriend(std::false_type{}, std::true_type{});
+  else befriend(std::false_type{}, std::false_type{});
   k_compress<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
   mark(3);
@@ -1496,6 +1591,23 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
     img += image_estimate(bd.g, sp.n);
   }
   if (n_total >= (int64_t)0xfffffff0ll) fail(CMH_ERR_CAPACITY, "more than 2^32 input particles in a run");
+  // linking-length tables of all boxes, one device array
+  varlink = false;
+  ltab_all.clear();
+  for (int b = 0; b < nbox; b++)
+    if (boxes_host[b].g.varlink) {
+      varlink = true;
+      ltab_all.insert(ltab_all.end(), specs[b].ltab.begin(), specs[b].ltab.end());
+    }
+  if (varlink) {
+    ltab_dev.ensure(ltab_all.size() * sizeof(double));
+    size_t off = 0;
+    for (int b = 0; b < nbox; b++)
+      if (boxes_host[b].g.varlink) {
+        boxes_host[b].g.ltab = ltab_dev.as<double>() + off;
+        off += specs[b].ltab.size();
+      }
+  }
   hs = 7 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
   k3all = (uint64_t)kmax * kmax * kmax;
   n_top = tops;
@@ -1526,6 +1638,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   const size_t rec = pos_dtype == CMH_FLOAT64 ? sizeof(SPos<double>) : sizeof(SPos<float>);
   b_ppos.ensure(npc * rec);
   b_spos.ensure(npc * rec);
+  if (varlink) b_svl.ensure(npc * sizeof(VLRec64));
   b_run_of.ensure(npc * 4);
   b_run_start.ensure((npc + 1) * 4);
   b_run_g.ensure(npc * 8);
@@ -1562,14 +1675,17 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   // cell (set here, outside any graph capture)
   {
     const int dsm = (int)(k3all * sizeof(uint32_t));
-    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<float, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<float, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<double, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-    CMH_CUDA(cudaFuncSetAttribute(k_befriend_dense<double, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+    const void *dense[] = {
+        (const void *)k_befriend_dense<float, true, false>,
+        (const void *)k_befriend_dense<float, false, false>,
+        (const void *)k_befriend_dense<double, true, false>,
+        (const void *)k_befriend_dense<double, false, false>,
+        (const void *)k_befriend_dense<float, true, true>,
+        (const void *)k_befriend_dense<float, false, true>,
+        (const void *)k_befriend_dense<double, true, true>,
+        (const void *)k_befriend_dense<double, false, true>};
+    for (const void *f : dense)
+      CMH_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
   }
   // pre-grow the scratch of the scans and sorts so that issue() allocates
   // nothing (it may be captured in a graph)
@@ -1649,10 +1765,15 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     const int64_t caps[6] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
                              (int64_t)dense_min};
     sig.insert(sig.end(), (const unsigned char *)caps, (const unsigned char *)caps + sizeof caps);
+    sig.insert(sig.end(), (const unsigned char *)ltab_all.data(),
+               (const unsigned char *)(ltab_all.data() + ltab_all.size()));
     const bool same = graph_exec && sig == graph_sig;
     if (!same) {
       CMH_CUDA(cudaMemcpyAsync(b_boxes.p, boxes_host.data(), sizeof(BoxDev) * boxes_host.size(),
                                cudaMemcpyHostToDevice, s));
+      if (varlink)
+        CMH_CUDA(cudaMemcpyAsync(ltab_dev.p, ltab_all.data(), ltab_all.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
       CMH_CUDA(cudaStreamSynchronize(s));
     }
     const long long l0 = g_launches;

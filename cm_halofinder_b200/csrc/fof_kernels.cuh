@@ -108,6 +108,79 @@ __host__ __device__ inline void band_thresholds(double l2, int ulps, float *t_lo
   *t_hi = fhi;
 }
 
+// ---- variable linking length (one value per cell of a fixed grid) ----
+//
+// The reference gives every cell of its fixed grid (Px x Py x Pz cells of
+// side lcell over the padded domain, FOF.c:45-52) one linking length, looked
+// up at the cell's distance from the observer (link.c:1-13,
+// FOF.c:102-109), and tests a pair with the length of the cell its scan
+// starts from: the lower of the two cells in (z, y, x) order, since each
+// cell scans itself and its 13 forward neighbours (FOF.c:111-153).  Pairs
+// whose cells are not neighbours are never tested.  Each processed particle
+// therefore carries its grid cell (packed z << 42 | y << 21 | x, which
+// orders like the scan) and that cell's l^2 (plain FP64 form) or FP32 band
+// (FP32 form; the band re-check recomputes l^2 from the cell).
+struct __align__(16) VLRec64 {
+  uint64_t rkey;
+  double lsq;
+};
+struct __align__(16) VLRec32 {
+  uint64_t rkey;
+  float t_lo, t_hi;
+};
+template <bool FP32> struct VLRecOf { using type = VLRec64; };
+template <> struct VLRecOf<true> { using type = VLRec32; };
+template <bool FP32> using VLRec = typename VLRecOf<FP32>::type;
+
+// Cell of the fixed grid holding (x, y, z): floor((x - rmin_buff) / lcell)
+// per axis, in double with IEEE division (FOF.c:76-92).
+__device__ __forceinline__ uint64_t ref_key(const Geom &g, double x, double y, double z) {
+  const double c[3] = {x, y, z};
+  uint64_t key = 0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    int i = (int)floor(__ddiv_rn(__dsub_rn(c[a], g.rmin[a]), g.ref_lcell[a]));
+    i = i < 0 ? 0 : (i > (1 << 21) - 1 ? (1 << 21) - 1 : i);
+    key |= (uint64_t)i << (21 * a);
+  }
+  return key;
+}
+
+// l^2 of a grid cell: the table l(r) (ltab_n values on r = 0, dr, ...,
+// rmax, linear in between, the last value beyond) at the distance of the
+// cell centre from the observer; every operation rounded as written.
+__device__ __forceinline__ double ref_cell_linksq(const Geom &g, uint64_t rkey) {
+  double q = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double i = (double)(int)((rkey >> (21 * a)) & 0x1fffffull);
+    const double c = __dadd_rn(__dsub_rn(g.rmin[a], g.origin[a]),
+                               __dmul_rn(__dadd_rn(i, 0.5), g.ref_lcell[a]));
+    q = a == 0 ? __dmul_rn(c, c) : __dadd_rn(q, __dmul_rn(c, c));
+  }
+  const double t = __ddiv_rn(__dsqrt_rn(q), g.ltab_dr);
+  double l;
+  if (t >= (double)(g.ltab_n - 1)) {
+    l = g.ltab[g.ltab_n - 1];
+  } else {
+    const int i = (int)t;
+    const double f = __dsub_rn(t, (double)i);
+    l = __dadd_rn(__dmul_rn(g.ltab[i], __dsub_rn(1.0, f)), __dmul_rn(g.ltab[i + 1], f));
+  }
+  return __dmul_rn(l, l);
+}
+
+// Whether two grid cells are equal or neighbours (|difference| <= 1 per axis).
+__device__ __forceinline__ bool ref_neighbours(uint64_t a, uint64_t b) {
+  bool ok = true;
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const int d = (int)((a >> (21 * s)) & 0x1fffffull) - (int)((b >> (21 * s)) & 0x1fffffull);
+    ok &= d >= -1 && d <= 1;
+  }
+  return ok;
+}
+
 // Fine-cell index along one axis: floor((x - rmin) * (1/h)), in double.  Two
 // points with the same index are within h (1 + 4e-16 * index) of each other
 // along the axis, far inside the 2^-20 margin that sizes h.

@@ -39,6 +39,8 @@ struct Plan : public cmh_plan {
   int64_t n_total = 0;
   uint64_t n_top = 0, k3all = 1;
   int key_bits = 0, hs = 7, props = 0;
+  bool varlink = false;             // some box has a variable linking length
+  std::vector<double> ltab_all;     // their tables, back to back
   int64_t np_cap = 0, nd_cap = 0, nc_cap = 0;  // grown on overflow, never shrunk
 
   // results of the last run
@@ -58,7 +60,7 @@ struct Plan : public cmh_plan {
   // workspace
   DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
   DevBuf b_keep, b_nimg, b_keep_scan, b_img_scan;
-  DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_run_of;
+  DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_svl, b_run_of;
   DevBuf b_run_start, b_run_g, b_run_box, b_top_first, b_top_end, b_top_slot, b_rtmp1, b_rtmp2;
   DevBuf b_maps, b_dense_range;
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;

@@ -11,6 +11,13 @@ Boundarysize 10).  The headline form is FP32 pair tests with FP64 re-check of
 the band; the plain FP64 form is measured on the same box and reported
 beside it.  With N GPUs (torchrun) every rank runs its own box (weak
 scaling; the boxes are independent domains, there is no exchange).
+Before timing, the plan's autotuner picks the cell-size scale and the
+dense-map threshold on the same box (--no-autotune keeps the defaults).
+
+Other workloads: --config c1 (64^3, FP64 positions), c3 (50M-particle
+lightcone with a variable linking length), c4 (64 batched boxes, 61M
+particles in one run), c5 (1024^3, generated on the device); --scale
+shrinks any of them.
 
 Timing: CUDA events on the launching stream, W untimed warm-up steps, K timed
 steps between barriers + synchronize; inputs (400 MB) exceed L2.
@@ -108,15 +115,15 @@ def make_workload(args, rank):
     raise SystemExit(f"unknown config {args.config}")
 
 
-def describe(args, w):
-    dt = "FP32" if w.pos.dtype == np.float32 else "FP64"
+def describe(args, w, dtype, n):
+    dt = "FP32" if dtype == np.float32 else "FP64"
     if getattr(w, "varlink", None):
         tab = w.varlink["table"]
         return (f"{args.config}: lightcone, sphere of radius {w.hi[0]:.1f} Mpc/h around the "
-                f"observer, N={w.n}, {dt} positions, {w.meta['n_clumps']} clumps, mean density "
+                f"observer, N={n}, {dt} positions, {w.meta['n_clumps']} clumps, mean density "
                 f"falling 3x outwards, l(r) from {tab.min():.4f} to {tab.max():.4f} on a "
                 f"{w.cells}^3 grid, non-periodic, Boundarysize={w.boundary}")
-    return (f"{args.config}: periodic box L={w.hi[0]:.1f} Mpc/h, N={w.n}, {dt} positions, "
+    return (f"{args.config}: periodic box L={w.hi[0]:.1f} Mpc/h, N={n}, {dt} positions, "
             f"{w.meta['n_clumps']} clumps, l={w.linklength:.6f}, Boundarysize={w.boundary}")
 
 
@@ -138,7 +145,7 @@ def stage_bytes(st, pos_bytes):
 
 def run_ours(args):
     import torch
-    from cm_halofinder_b200 import FofConfig, Plan
+    from cm_halofinder_b200 import FofConfig, Plan, synth
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -150,11 +157,19 @@ def run_ours(args):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    w = make_workload(args, rank)
-    n = w.n
     dev = torch.device("cuda", local)
-    pos = torch.from_numpy(w.pos).to(dev)
-    vel = torch.from_numpy(w.vel).to(dev)
+    if args.config == "c5":
+        # 1024^3: drawn on the device (host generation would take minutes)
+        w = synth.config5_device(seed=5 + rank, scale=args.scale, device=local)
+        pos, vel = w.pos, w.vel
+        w.pos = w.vel = None
+    else:
+        w = make_workload(args, rank)
+        pos = torch.from_numpy(w.pos).to(dev)
+        vel = torch.from_numpy(w.vel).to(dev)
+    n = int(pos.shape[0])
+    np_dtype = np.float32 if pos.dtype == torch.float32 else np.float64
+    in_bytes = pos.numel() * pos.element_size() + vel.numel() * vel.element_size()
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -162,29 +177,28 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
+    def max_ranks(ms):
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
     def timed(plan, steps, warmup):
         for _ in range(warmup):
             plan.run(pos, vel, out="device", stream=stream)
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        stages = {}
         launches = 0
         e0.record(stream)
         for _ in range(steps):
             cat = plan.run(pos, vel, out="device", stream=stream)
             st = cat.stats.as_dict()
             launches += st["n_launches"]
-            for k, v in st["stage_ms"].items():
-                stages[k] = stages.get(k, 0.0) + v / steps
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1) / steps
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, st, stages, launches
+        return max_ranks(e0.elapsed_time(e1) / steps), st, launches
 
     def stage_breakdown(plan):
         # one eager (non-graph) step: the library records CUDA events between
@@ -194,34 +208,65 @@ def run_ours(args):
         plan.set_graph(not args.no_graph)
         return cat.stats.as_dict()["stage_ms"]
 
+    # the chosen form; each plan is closed after its leg so that the largest
+    # workload holds one plan's buffers at a time
     cfg_fast = FofConfig.from_workload(w, precision=args.precision)
-    plan = Plan(cfg_fast, pos_dtype=w.pos.dtype, device=local)
+    plan = Plan(cfg_fast, pos_dtype=np_dtype, device=local)
     plan.set_graph(not args.no_graph)
+    tune = None
+    if not args.no_autotune:
+        tune = plan.autotune([cfg_fast], [pos], [vel], repeats=2, stream=stream)
     clocks = ClockSampler(local)
     for _ in range(args.warmup):
         plan.run(pos, vel, out="device", stream=stream)
     clocks.start()
-    ms, st, _, launches = timed(plan, args.steps, 0)
+    ms, st, launches = timed(plan, args.steps, 0)
     clk = clocks.stop()
     stages = stage_breakdown(plan)
     value = n * world / (ms * 1e-3) / 1e6
+    cat_fast = plan.run(pos, vel, out="host", stream=stream)
+    plan.close()
 
     plain = None
     if not args.no_plain and args.precision != "fp64":
-        plan_p = Plan(FofConfig.from_workload(w, precision="fp64"), pos_dtype=w.pos.dtype,
-                      device=local)
+        cfg_p = FofConfig.from_workload(w, precision="fp64")
+        plan_p = Plan(cfg_p, pos_dtype=np_dtype, device=local)
         plan_p.set_graph(not args.no_graph)
-        ms_p, st_p, _, _ = timed(plan_p, max(1, args.steps), args.warmup)
+        if tune is not None:
+            plan_p.set_tuning(tune)
+        ms_p, st_p, _ = timed(plan_p, max(1, args.steps), args.warmup)
         stages_p = stage_breakdown(plan_p)
+        cat_p = plan_p.run(pos, vel, out="host", stream=stream)
+        plan_p.close()
+        # size-independent parity at full size: the two forms give the same
+        # halos (heads, member counts) and properties within 1e-6
+        same = (cat_p.nhalos == cat_fast.nhalos and
+                np.array_equal(cat_p.head, cat_fast.head) and
+                np.array_equal(cat_p.props[:, 0], cat_fast.props[:, 0]))
+        rel = 0.0
+        if same and cat_p.nhalos:
+            a = cat_p.props[:, 1:4].astype(np.float64)
+            b = cat_fast.props[:, 1:4].astype(np.float64)
+            rel = float(np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-30)))
         plain = {"value": n * world / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
                  "n_pair_tests": st_p["n_pair_tests"],
                  "stage_ms": {k: round(v, 4) for k, v in stages_p.items()},
-                 "speedup_of_chosen_form": ms_p / ms}
-        plan_p.close()
+                 "speedup_of_chosen_form": ms_p / ms,
+                 "same_halos_as_chosen_form": bool(same), "max_rel_diff_com": rel}
 
     # end to end through the public API: pinned host inputs, catalog back
-    pin_pos = torch.from_numpy(w.pos).pin_memory().numpy()
-    pin_vel = torch.from_numpy(w.vel).pin_memory().numpy()
+    pin_pos = torch.empty(tuple(pos.shape), dtype=pos.dtype, pin_memory=True)
+    pin_vel = torch.empty(tuple(vel.shape), dtype=vel.dtype, pin_memory=True)
+    pin_pos.copy_(pos)
+    pin_vel.copy_(vel)
+    if args.config == "c5":
+        pos = vel = None          # the plan copies the host inputs into its own buffers
+        torch.cuda.empty_cache()
+    pin_pos, pin_vel = pin_pos.numpy(), pin_vel.numpy()
+    plan = Plan(cfg_fast, pos_dtype=np_dtype, device=local)
+    plan.set_graph(not args.no_graph)
+    if tune is not None:
+        plan.set_tuning(tune)
     for _ in range(max(1, args.warmup)):
         plan.run(pin_pos, pin_vel, out="host", stream=stream)
     barrier()
@@ -234,16 +279,13 @@ def run_ours(args):
         d2h = hc.props.nbytes + hc.head.nbytes
     e1.record(stream)
     barrier()
-    ms_e2e = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    plan.close()
+    ms_e2e = max_ranks(e0.elapsed_time(e1) / args.steps)
     e2e = {"value": n * world / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
-           "h2d_bytes_per_step": int(w.pos.nbytes + w.vel.nbytes), "d2h_bytes_per_step": int(d2h)}
+           "h2d_bytes_per_step": int(in_bytes), "d2h_bytes_per_step": int(d2h)}
 
     peak, peak_kind = peaks()
-    pos_bytes = w.pos.dtype.itemsize
+    pos_bytes = np.dtype(np_dtype).itemsize
     sb = stage_bytes(st, pos_bytes)
     dominant = max(sb, key=lambda k: stages.get(k, 0.0))
     ach = sb[dominant] / (stages[dominant] * 1e-3) / 1e9
@@ -256,7 +298,12 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, args.cpu_seconds)
+        if args.config == "c5":
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": "not run for the 1024^3 box (the sampled sub-domains of the "
+                             "256^3 box give the reference's rate)"}
+        else:
+            cpu = cpu_baseline(w, args.cpu_seconds)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -268,7 +315,7 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64-recheck" if args.precision == "fp32" else "f64",
         "data": "synthetic (seeded Plummer clumps + uniform background)",
-        "config": {"workload": describe(args, w),
+        "config": {"workload": describe(args, w, np_dtype, n),
                    "n_particles": n, "n_processed": st["n_proc"], "n_images": st["n_images"],
                    "n_halos": st["nhalos"], "n_groups": st["n_groups"],
                    "n_fine_cells": st["n_cells"], "cell_factor": st["cell_factor"],
@@ -276,10 +323,9 @@ def run_ours(args):
                    "cell_pairs": st["n_cell_pairs"], "root_skips": st["n_root_skips"],
                    "unions": st["n_unions"], "find_steps": st["n_find_steps"],
                    "scan_iters": st["n_scan_iters"], "window_iters": st["n_window_iters"],
-                   "dense_tops": st["n_dense_tops"],
+                   "dense_tops": st["n_dense_tops"], "autotune": tune,
                    "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": f"inputs ({(w.pos.nbytes + w.vel.nbytes) / 1e6:.0f} MB) larger than "
-                         "L2; no flush"},
+                   "l2": f"inputs ({in_bytes / 1e6:.0f} MB) larger than L2; no flush"},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "stage_ms_note": "per-stage CUDA-event times of one eager step after the timed graph replays",
         "plain_fp64": plain,
@@ -526,7 +572,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="issue every step eagerly")
-    ap.add_argument("--no-autotune", action="store_true", help="batched boxes: default cell sizes")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the autotuner (default cell-size factor and dense-map threshold)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-timeout", type=float, default=20.0)
     ap.add_argument("--traffic", type=float, default=None,

@@ -250,6 +250,12 @@ class Plan:
         return {"cell_scale": t.cell_scale, "dense_min": t.dense_min, "ms": t.ms,
                 "tried": t.tried}
 
+    def set_tuning(self, tuning):
+        """Apply a setting returned by autotune() (e.g. to a new plan)."""
+        t = _abi.Tuning(cell_scale=float(tuning["cell_scale"]),
+                        dense_min=int(tuning["dense_min"]))
+        _abi.check(self._L.cmh_plan_set_tuning(self._h, C.byref(t)))
+
     def run_batch(self, configs, positions, velocities, stream=None):
         """Many independent boxes in one run (one sort, one befriending pass,
         one reduction for all of them); positions/velocities are torch CUDA

@@ -107,6 +107,7 @@ SIGNATURES = {
     "cmh_plan_set_graph": (C.c_int, [C.c_void_p, C.c_int32]),
     "cmh_plan_autotune": (C.c_int, [C.c_void_p, C.POINTER(FofParams), C.POINTER(Particles),
                                     C.c_int32, C.c_int32, C.c_void_p, C.POINTER(Tuning)]),
+    "cmh_plan_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "cmh_plan_run_batch": (C.c_int, [C.c_void_p, C.POINTER(FofParams), C.POINTER(Particles),
                                      C.c_int32, C.POINTER(Catalog), C.c_void_p]),
     "cmh_fof_run_batch": (C.c_int, [C.POINTER(FofParams), C.POINTER(Particles), C.c_int32,

@@ -39,8 +39,15 @@ void DevBuf::ensure(size_t bytes) {
   if (p) CMH_CUDA(cudaFree(p));
   p = nullptr;
   cap = 0;
-  size_t want = bytes + bytes / 8 + 256;  // headroom against small regrowth
-  CMH_CUDA(cudaMalloc(&p, want));
+  size_t want = bytes + bytes / 64 + 256;  // headroom against small regrowth
+  const cudaError_t e = cudaMalloc(&p, want);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    p = nullptr;
+    fail(CMH_ERR_OUT_OF_MEMORY, "device memory exhausted (" + std::to_string(want >> 20) +
+                                    " MiB requested)");
+  }
+  CMH_CUDA(e);
   cap = want;
 }
 
@@ -65,19 +72,20 @@ Plan::~Plan() {
   cudaSetDevice(device);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (cap_stream) cudaStreamDestroy(cap_stream);
-  DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd, &b_keep,
-                   &b_nimg, &b_keep_scan, &b_img_scan, &b_keys, &b_keys_alt, &b_vals,
-                   &b_vals_alt, &b_ppos, &b_spos, &b_svl, &b_run_of, &b_run_start, &b_run_g,
-                   &b_run_box, &b_top_first, &b_top_end, &b_top_slot, &b_rtmp1, &b_rtmp2,
-                   &b_maps, &b_dense_range, &b_parent, &b_count, &b_head, &b_cand_of_root,
-                   &b_cand_root, &b_sums, &b_warn, &b_own, &b_own_scan, &b_okeys, &b_ovals,
-                   &b_okeys_alt, &b_ovals_alt, &b_props, &b_head_out, &b_cat_of_cand,
-                   &b_member, &b_member_proc, &b_member_pos, &in_pos, &in_vel};
-  for (DevBuf *b : all) b->release();
+  each_buf([](DevBuf &b) { b.release(); });
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   for (cudaEvent_t e : stage_ev)
     if (e) cudaEventDestroy(e);
+}
+
+void Plan::release_workspace() {
+  cudaSetDevice(device);
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  graph_exec = nullptr;
+  graph_sig.clear();
+  each_buf([](DevBuf &b) { b.release(); });
+  np_cap = nd_cap = nc_cap = 0;
 }
 
 void Plan::set_params(const cmh_fof_params &p) {
@@ -371,6 +379,17 @@ cmh_status cmh_plan_autotune(cmh_plan *plan, const cmh_fof_params *params,
   cmh_tuning t = pl.autotune(make_specs(pl, params, parts, nbox), repeats,
                              static_cast<cudaStream_t>(stream));
   if (out) *out = t;
+  CMH_API_END
+}
+
+cmh_status cmh_plan_set_tuning(cmh_plan *plan, const cmh_tuning *tuning) {
+  CMH_API_BEGIN
+  if (!plan || !tuning) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and tuning are required");
+  if (!(tuning->cell_scale > 0) || tuning->cell_scale > 64 || tuning->dense_min < 1)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "cell_scale must be in (0, 64] and dense_min >= 1");
+  Plan &pl = *static_cast<Plan *>(plan);
+  pl.cell_scale = tuning->cell_scale;
+  pl.dense_min = (uint32_t)tuning->dense_min;
   CMH_API_END
 }
 

@@ -197,7 +197,10 @@ __device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint6
 // Processing order of a box: kept originals in input order, then the images
 // grouped by source particle and shift code (sz+1)*9 + (sy+1)*3 + (sx+1)
 // ascending.  Writes beyond the capacity are dropped (the run is then
-// repeated with more room).
+// repeated with more room).  A warp walks 32 consecutive particles; the
+// images of each particle that has some are then emitted by the whole warp
+// at once, one shift code per lane, so that the few image particles do not
+// hold the other lanes through a 27-step loop.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_ingest_emit(
     const BoxDev *__restrict__ boxes, int nbox, int64_t n, uint64_t k3all,
@@ -207,39 +210,47 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
     uint32_t *__restrict__ vals, SPos<PT> *__restrict__ ppos) {
   __shared__ uint64_t s_base[kMaxBoxes];
   load_bases(boxes, nbox, s_base, false);
-  for (int64_t i = gtid(); i < n; i += gstride()) {
-    if (!keep[i]) continue;
-    const int b = box_search(s_base, nbox, (uint64_t)i);
-    const BoxDev &bx = boxes[b];
-    const Geom &g = bx.g;
-    double x[3];
-    load_pos<PT>(bx, (uint64_t)i - bx.in_base, x);
-    const uint32_t pbase = boxd[4 * nbox + b];
-    const uint32_t p = pbase + (keep_scan[i] - boxd[0 * nbox + b]);
-    if (p < np_cap) emit_one<PT>(g, bx.top_base, k3all, p, x, (uint32_t)i, keys, vals, ppos);
-    if (!g.periodic || nimg[i] == 0) continue;
-    uint32_t q = pbase + boxd[2 * nbox + b] + (img_scan[i] - boxd[1 * nbox + b]);
-    double cm[3], cp[3];
-    bool okm[3], okp[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      okm[a] = image_coord<PT>(g, x[a], a, -1, &cm[a]);
-      okp[a] = image_coord<PT>(g, x[a], a, 1, &cp[a]);
+  const int lane = threadIdx.x & 31;
+  for (int64_t w0 = gtid() - lane; w0 < n; w0 += gstride()) {
+    const int64_t i = w0 + lane;
+    int b = 0;
+    double x[3] = {0.0, 0.0, 0.0};
+    uint32_t q0 = 0;
+    bool has_img = false;
+    if (i < n && keep[i]) {
+      b = box_search(s_base, nbox, (uint64_t)i);
+      const BoxDev &bx = boxes[b];
+      load_pos<PT>(bx, (uint64_t)i - bx.in_base, x);
+      const uint32_t pbase = boxd[4 * nbox + b];
+      const uint32_t p = pbase + (keep_scan[i] - boxd[0 * nbox + b]);
+      if (p < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, p, x, (uint32_t)i, keys, vals, ppos);
+      if (bx.g.periodic && nimg[i] != 0) {
+        has_img = true;
+        q0 = pbase + boxd[2 * nbox + b] + (img_scan[i] - boxd[1 * nbox + b]);
+      }
     }
-    for (int code = 0; code < 27; code++) {
-      if (code == 13) continue;
-      const int s[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+    unsigned m = __ballot_sync(0xffffffffu, has_img);
+    while (m) {
+      const int src = __ffs(m) - 1;
+      m &= m - 1;
+      const int64_t si = __shfl_sync(0xffffffffu, i, src);
+      const int sb = __shfl_sync(0xffffffffu, b, src);
+      const uint32_t sq = __shfl_sync(0xffffffffu, q0, src);
+      double sx[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) sx[a] = __shfl_sync(0xffffffffu, x[a], src);
+      const BoxDev &bx = boxes[sb];
+      const int sh[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+      bool ok = lane < 27 && lane != 13;
       double c[3];
-      bool ok = true;
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        if (s[a] < 0) { ok &= okm[a]; c[a] = cm[a]; }
-        else if (s[a] > 0) { ok &= okp[a]; c[a] = cp[a]; }
-        else c[a] = x[a];
+        c[a] = sx[a];
+        if (ok && sh[a] != 0) ok = image_coord<PT>(bx.g, sx[a], a, sh[a], &c[a]);
       }
-      if (!ok) continue;
-      if (q < np_cap) emit_one<PT>(g, bx.top_base, k3all, q, c, (uint32_t)i, keys, vals, ppos);
-      q++;
+      const unsigned vm = __ballot_sync(0xffffffffu, ok);
+      const uint32_t q = sq + (uint32_t)__popc(vm & ((1u << lane) - 1u));
+      if (ok && q < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, q, c, (uint32_t)si, keys, vals, ppos);
     }
   }
 }
@@ -381,8 +392,13 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
   }
 }
 
+// Dense top cells with more fine cells than this are joined by a whole CTA,
+// the others by one warp each.
+constexpr uint32_t kBigTop = 128;
+
 // Fine-cell maps of the dense top cells (the first nd_cap of them; a dense
 // top cell without a map is scanned instead, which is slower but exact).
+// The slots of the big ones are listed in `big`.
 __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ run_g,
                                                    const uint16_t *__restrict__ run_box,
                                                    const BoxDev *__restrict__ boxes,
@@ -394,6 +410,7 @@ __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ 
                                                    uint32_t dense_min, uint32_t nd_cap,
                                                    uint32_t *__restrict__ top_slot,
                                                    uint2 *__restrict__ dense_range,
+                                                   uint32_t *__restrict__ big,
                                                    int32_t *__restrict__ maps) {
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
@@ -407,6 +424,7 @@ __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ 
     if (dflag[r]) {
       top_slot[t] = slot;
       dense_range[slot] = make_uint2(f, top_end[t]);
+      if (top_end[t] - f > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
     }
     const int k = bx.g.k;
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
@@ -613,72 +631,108 @@ __device__ __forceinline__ void lunion(uint32_t *lp, uint32_t a, uint32_t b, Cou
   atomicAdd(&ctr->uf_giveups, 1u);
 }
 
-// Dense top cells, one CTA each: the fine-cell pairs inside the top cell are
-// joined with a shared-memory union-find (neighbours found through the top
-// cell's fine-cell map), near pairs before far ones; then every fine cell's
-// global parent is set to its local root.  Links that cross the top cell's
-// faces are left to the global passes.  CTAs take top cells from an atomic
-// counter: their sizes differ widely.
+// Dense top cells: the fine-cell pairs inside a top cell are joined with a
+// union-find in shared memory (neighbours found through the top cell's
+// fine-cell map), near pairs before far ones; then every fine cell's global
+// parent is set to its local root.  Links that cross the top cell's faces
+// are left to the global passes.  `tid`/`nt` number the threads that share
+// the top cell and `sync` is their barrier.
+template <class PT, bool FP32, bool VL, class Sync>
+__device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_t tid,
+                                          uint32_t nt, Sync sync, const BoxDev *boxes,
+                                          const uint16_t *run_box, uint64_t k3all,
+                                          const uint32_t *run_start, const uint64_t *run_g,
+                                          const uint2 *dense_range, const int32_t *maps,
+                                          const SPos<PT> *spos, const VLRec<FP32> *svl,
+                                          uint32_t *parent, Counters *ctr, BfStats &st) {
+  const uint2 fr = dense_range[slot];
+  const uint32_t f = fr.x, n = fr.y - fr.x;
+  const Geom &g = boxes[run_box[f]].g;
+  const int k = g.k, W = g.W;
+  for (uint32_t i = tid; i < n; i += nt) lpar[i] = i;
+  sync();
+  const int32_t *map = maps + (uint64_t)slot * k3all;
+  for (int pass = 0; pass < 2; pass++) {
+    for (uint32_t i = tid; i < n; i += nt) {
+      const uint32_t a = f + i;
+      const uint64_t pg = run_g[a];
+      const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
+      const int sx = gx % k, sy = gy % k, sz = gz % k;
+      const uint32_t sa = run_start[a], ea = run_start[a + 1];
+      for (int dz = 0; dz <= W; dz++)
+        for (int dy = -W; dy <= W; dy++)
+          for (int dx = -W; dx <= W; dx++) {
+            if (dz == 0 && (dy < 0 || (dy == 0 && dx <= 0))) continue;  // forward only
+            const int cheb = max(abs(dx), max(abs(dy), dz));
+            if ((pass == 0) != (cheb <= 1)) continue;
+            const int tx = sx + dx, ty = sy + dy, tz = sz + dz;
+            if (tx < 0 || ty < 0 || tx >= k || ty >= k || tz >= k) continue;
+            const int32_t r = map[(tz * k + ty) * k + tx];
+            if (r < 0) continue;
+            st.cand++;
+            const uint32_t lj = (uint32_t)r - f;
+            const uint32_t ri = lfind(lpar, i), rj = lfind(lpar, lj);
+            if (ri == rj) {
+              st.skips++;
+              continue;
+            }
+            auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
+            if (cells_linked<PT, FP32, VL>(g, (uint32_t)r, gx + dx, gy + dy, gz + dz, sa, ea,
+                                           run_start, spos, svl, st, apart)) {
+              lunion(lpar, ri, rj, ctr);
+              st.unions++;
+            }
+          }
+    }
+    sync();
+  }
+  for (uint32_t i = tid; i < n; i += nt) parent[f + i] = f + lfind(lpar, i);
+  sync();
+}
+
+// The dense top cells.  The big ones (more than kBigTop fine cells, listed
+// in `big`) go first, one per CTA, so that the largest, which bound the
+// kernel's length, start early and have many threads; then each warp takes
+// the small ones one at a time, with its own slice of `lstride` parents of
+// shared memory.  Both kinds are taken from atomic counters: their sizes
+// differ widely.
 template <class PT, bool FP32, bool VL>
 __global__ void __launch_bounds__(128) k_befriend_dense(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
-    const uint2 *__restrict__ dense_range, DevScal *sc, uint32_t nd_cap,
-    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
-    const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr) {
-  extern __shared__ uint32_t lpar[];
+    const uint2 *__restrict__ dense_range, const uint32_t *__restrict__ big, DevScal *sc,
+    uint32_t nd_cap, const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
+    const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr, uint32_t lstride) {
+  extern __shared__ uint32_t smem[];
   __shared__ uint32_t s_slot;
-  const uint32_t nd = min(sc->nd, nd_cap);
+  const uint32_t nd = min(sc->nd, nd_cap), nbig = sc->nbig;
   BfStats st;
+  auto cta_sync = []() { __syncthreads(); };
   while (true) {
-    if (threadIdx.x == 0) s_slot = atomicAdd(&sc->next_dense, 1u);
+    if (threadIdx.x == 0) {
+      const uint32_t b = atomicAdd(&sc->next_big, 1u);
+      s_slot = b < nbig ? big[b] : kNone;
+    }
     __syncthreads();
     const uint32_t slot = s_slot;
     __syncthreads();
+    if (slot == kNone) break;
+    dense_top<PT, FP32, VL>(slot, smem, threadIdx.x, blockDim.x, cta_sync, boxes, run_box,
+                            k3all, run_start, run_g, dense_range, maps, spos, svl, parent,
+                            ctr, st);
+  }
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t *lpar = smem + (size_t)(threadIdx.x >> 5) * lstride;
+  auto warp_sync = []() { __syncwarp(); };
+  while (true) {
+    uint32_t slot = 0;
+    if (lane == 0) slot = atomicAdd(&sc->next_dense, 1u);
+    slot = __shfl_sync(0xffffffffu, slot, 0);
     if (slot >= nd) break;
     const uint2 fr = dense_range[slot];
-    const uint32_t f = fr.x, n = fr.y - fr.x;
-    const Geom &g = boxes[run_box[f]].g;
-    const int k = g.k, W = g.W;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) lpar[i] = i;
-    __syncthreads();
-    const int32_t *map = maps + (uint64_t)slot * k3all;
-    for (int pass = 0; pass < 2; pass++) {
-      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t a = f + i;
-        const uint64_t pg = run_g[a];
-        const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-        const int sx = gx % k, sy = gy % k, sz = gz % k;
-        const uint32_t sa = run_start[a], ea = run_start[a + 1];
-        for (int dz = 0; dz <= W; dz++)
-          for (int dy = -W; dy <= W; dy++)
-            for (int dx = -W; dx <= W; dx++) {
-              if (dz == 0 && (dy < 0 || (dy == 0 && dx <= 0))) continue;  // forward only
-              const int cheb = max(abs(dx), max(abs(dy), dz));
-              if ((pass == 0) != (cheb <= 1)) continue;
-              const int tx = sx + dx, ty = sy + dy, tz = sz + dz;
-              if (tx < 0 || ty < 0 || tx >= k || ty >= k || tz >= k) continue;
-              const int32_t r = map[(tz * k + ty) * k + tx];
-              if (r < 0) continue;
-              st.cand++;
-              const uint32_t lj = (uint32_t)r - f;
-              const uint32_t ri = lfind(lpar, i), rj = lfind(lpar, lj);
-              if (ri == rj) {
-                st.skips++;
-                continue;
-              }
-              auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
-              if (cells_linked<PT, FP32, VL>(g, (uint32_t)r, gx + dx, gy + dy, gz + dz, sa,
-                                             ea, run_start, spos, svl, st, apart)) {
-                lunion(lpar, ri, rj, ctr);
-                st.unions++;
-              }
-            }
-      }
-      __syncthreads();
-    }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) parent[f + i] = f + lfind(lpar, i);
-    __syncthreads();
+    if (fr.y - fr.x > kBigTop) continue;
+    dense_top<PT, FP32, VL>(slot, lpar, lane, 32, warp_sync, boxes, run_box, k3all, run_start,
+                            run_g, dense_range, maps, spos, svl, parent, ctr, st);
   }
   st.flush(ctr);
 }
@@ -698,7 +752,7 @@ __device__ __forceinline__ bool reaches(int s, int o, int k, int W) {
 // (the common case away from clumps), the first of each is loaded at once too
 // and the cell is finished in two L2 round trips.  Other cells are queued for
 // the warp path below.
-constexpr uint32_t kSimple = 2;
+constexpr uint32_t kSimple = 2;  // two slot bits per range below
 
 template <class PT, bool FP32, bool VL>
 __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
@@ -748,25 +802,39 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
       if (!simple) queue[base + __popc(qmask & ((1u << lane) - 1u))] = a;
     }
     if (!simple) continue;
-    uint64_t Q[14];
-#pragma unroll
-    for (int nb = 0; nb < 14; nb++) Q[nb] = NN[nb] ? run_g[R0[nb]] : 0ull;
-    uint32_t ra = 0xffffffffu, sa = 0, ea = 0;
+    // candidate slots: bit 2 nb + q stands for fine cell R0[nb] + q.  The
+    // first fine cell of every range is loaded at once and dropped here when
+    // out of reach; the slots left are visited from one call site below (a
+    // single inlined copy of the link test keeps the kernel's code small)
+    uint32_t m = 0;
 #pragma unroll
     for (int nb = 0; nb < 14; nb++) {
-      for (uint32_t q = 0; q < NN[nb]; q++) {
-        const uint64_t qg = q == 0 ? Q[nb] : run_g[R0[nb] + q];
-        const int bx2 = (int)(qg & kM21), by2 = (int)((qg >> 21) & kM21), bz2 = (int)(qg >> 42);
-        st.scan++;
-        if (max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz))) > W) continue;
-        if (ra == 0xffffffffu) {
-          ra = __ldcg(parent + a);
-          sa = run_start[a];
-          ea = run_start[a + 1];
-        }
-        try_link<PT, FP32, VL>(g, a, ra, R0[nb] + q, bx2, by2, bz2, sa, ea, run_start, spos, svl,
-                               parent, ctr, st);
+      if (NN[nb] == 0) continue;
+      st.scan += NN[nb];
+      const uint64_t qg = run_g[R0[nb]];
+      const int bx2 = (int)(qg & kM21), by2 = (int)((qg >> 21) & kM21), bz2 = (int)(qg >> 42);
+      if (max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz))) <= W) m |= 1u << (2 * nb);
+      if (NN[nb] > 1) m |= 2u << (2 * nb);
+    }
+    uint32_t ra = 0xffffffffu, sa = 0, ea = 0;
+    while (m) {
+      const int bit = __ffs(m) - 1;
+      m &= m - 1;
+      const int nb = bit >> 1;
+      uint32_t r = 0;
+#pragma unroll
+      for (int t = 0; t < 14; t++) r = t == nb ? R0[t] : r;
+      r += (uint32_t)(bit & 1);
+      const uint64_t qg = run_g[r];  // L1 hit for the first cell of a range
+      const int bx2 = (int)(qg & kM21), by2 = (int)((qg >> 21) & kM21), bz2 = (int)(qg >> 42);
+      if ((bit & 1) && max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz))) > W) continue;
+      if (ra == 0xffffffffu) {
+        ra = __ldcg(parent + a);
+        sa = run_start[a];
+        ea = run_start[a + 1];
       }
+      try_link<PT, FP32, VL>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent,
+                             ctr, st);
     }
   }
   st.flush(ctr);
@@ -1335,6 +1403,19 @@ Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &lta
 }
 
 namespace {
+// Warps per CTA of the dense-top kernel: up to 4, each with k^3 parents of
+// shared memory, within 200 KiB per CTA.
+int dense_warps_per_cta(uint64_t k3all) {
+  const uint64_t per = k3all * sizeof(uint32_t);
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>(4, (200u << 10) / per));
+}
+
+// Dense top cells whose fine-cell maps fit in 8 bytes per processed particle
+// plus 1 GiB.
+int64_t maps_cap_for(int64_t np_cap, uint64_t k3all) {
+  return (int64_t)(((uint64_t)np_cap * 8 + (1ull << 30)) / (k3all * 4));
+}
+
 // Images per input particle expected for a periodic box (the shell's share
 // of the padded volume), with headroom for clustering.
 double image_estimate(const Geom &g, int64_t n) {
@@ -1354,6 +1435,13 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   unsigned long long *extra = reinterpret_cast<unsigned long long *>(c + 1);  // ngroups, nwarn
   uint32_t *boxd = b_boxd.as<uint32_t>();
   const BoxDev *boxes = b_boxes.as<BoxDev>();
+  // buffers whose lifetimes do not overlap share memory: the ingest flags and
+  // scans live in arrays of the group stage, and the fine-cell tables run_g
+  // and run_of in the unsorted positions, which are dead after the gather
+  uint32_t *keep = b_count.as<uint32_t>(), *nimg = b_head.as<uint32_t>();
+  uint32_t *keep_scan = b_rtmp1.as<uint32_t>(), *img_scan = b_rtmp2.as<uint32_t>();
+  uint64_t *run_g = b_ppos.as<uint64_t>();
+  uint32_t *run_of = reinterpret_cast<uint32_t *>(run_g + npc);
   auto mark = [&](int q) {
     if (timed) CMH_CUDA(cudaEventRecord(q < 0 ? ev0 : (q >= 7 ? ev1 : stage_ev[q]), s));
   };
@@ -1364,21 +1452,21 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 
   // ---- ingest ----
   if (n > 0) {
-    k_ingest_count<PT><<<grid_for(n, kT), kT, 0, s>>>(boxes, nbox, n, b_keep.as<uint32_t>(),
-                                                      b_nimg.as<uint32_t>());
+    k_ingest_count<PT><<<grid_for(n, kT), kT, 0, s>>>(boxes, nbox, n, keep,
+                                                      nimg);
     CMH_LAUNCHED();
   }
-  exclusive_scan_u32(b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(), n, &sc->kept_total,
+  exclusive_scan_u32(keep, keep_scan, n, &sc->kept_total,
                      scan_tmp, s);
-  exclusive_scan_u32(b_nimg.as<uint32_t>(), b_img_scan.as<uint32_t>(), n, &sc->img_total,
+  exclusive_scan_u32(nimg, img_scan, n, &sc->img_total,
                      scan_tmp, s);
-  k_box_totals<<<1, 32, 0, s>>>(boxes, nbox, n, b_keep_scan.as<uint32_t>(),
-                                b_img_scan.as<uint32_t>(), sc, boxd, (uint32_t)npc);
+  k_box_totals<<<1, 32, 0, s>>>(boxes, nbox, n, keep_scan,
+                                img_scan, sc, boxd, (uint32_t)npc);
   CMH_LAUNCHED();
   if (n > 0) {
     k_ingest_emit<PT><<<grid_for(n, kT), kT, 0, s>>>(
-        boxes, nbox, n, k3all, b_keep.as<uint32_t>(), b_keep_scan.as<uint32_t>(),
-        b_img_scan.as<uint32_t>(), b_nimg.as<uint32_t>(), boxd, (uint32_t)npc,
+        boxes, nbox, n, k3all, keep, keep_scan,
+        img_scan, nimg, boxd, (uint32_t)npc,
         b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
     CMH_LAUNCHED();
   }
@@ -1397,16 +1485,16 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s);
   k_runs<<<gp, kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, boxes, nbox, k3all, sc,
-                           b_run_of.as<uint32_t>(), b_run_start.as<uint32_t>(),
-                           b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>());
+                           run_of, b_run_start.as<uint32_t>(),
+                           run_g, b_run_box.as<uint16_t>());
   CMH_LAUNCHED();
   if (varlink) {
     if (fp32)
-      k_varlink_recs<PT, true><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), b_run_of.as<uint32_t>(),
+      k_varlink_recs<PT, true><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
                                                  b_run_box.as<uint16_t>(), boxes, sc,
                                                  b_svl.as<VLRec32>());
     else
-      k_varlink_recs<PT, false><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), b_run_of.as<uint32_t>(),
+      k_varlink_recs<PT, false><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
                                                   b_run_box.as<uint16_t>(), boxes, sc,
                                                   b_svl.as<VLRec64>());
     CMH_LAUNCHED();
@@ -1414,10 +1502,10 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaMemsetAsync(b_top_first.p, 0, n_top * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_top_end.p, 0, n_top * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, s));
-  k_top_ranges<<<gp, kT, 0, s>>>(b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+  k_top_ranges<<<gp, kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
                                  b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>());
   CMH_LAUNCHED();
-  k_dense_flags<<<gp, kT, 0, s>>>(b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+  k_dense_flags<<<gp, kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
                                   npc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(),
                                   dense_min, b_rtmp1.as<uint32_t>());
   CMH_LAUNCHED();
@@ -1425,11 +1513,12 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   k_clamp_dense<<<1, 32, 0, s>>>(sc, (uint32_t)nd_cap);
   CMH_LAUNCHED();
   CMH_CUDA(cudaMemsetAsync(b_maps.p, 0xff, (size_t)nd_cap * k3all * 4, s));
-  k_dense_maps<<<gp, kT, 0, s>>>(b_run_g.as<uint64_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+  k_dense_maps<<<gp, kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
                                  k3all, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(),
                                  b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), dense_min,
                                  (uint32_t)nd_cap, b_top_slot.as<uint32_t>(),
-                                 b_dense_range.as<uint2>(), b_maps.as<int32_t>());
+                                 b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(),
+                                 b_maps.as<int32_t>());
   CMH_LAUNCHED();
   k_iota<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
@@ -1438,25 +1527,28 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   // warp path near then far ----
   uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
   const unsigned gw = grid_for(npc * 32, kT);
-  const size_t dsm = (size_t)k3all * sizeof(uint32_t);
-  const unsigned gd = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nd_cap, (int64_t)kSMs * 16));
+  const int dwpc = dense_warps_per_cta(k3all);
+  const size_t dsm = (size_t)dwpc * k3all * sizeof(uint32_t);
+  const unsigned gd = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>((nd_cap + dwpc - 1) / dwpc, (int64_t)kSMs * 64 / dwpc));
   auto befriend = [&](auto fp32_tag, auto vl_tag) {
     constexpr bool FP = decltype(fp32_tag)::value;
     constexpr bool VL = decltype(vl_tag)::value;
     const VLRec<FP> *svl = VL ? b_svl.as<VLRec<FP>>() : nullptr;
-    k_befriend_dense<PT, FP, VL><<<gd, 128, dsm, s>>>(
+    k_befriend_dense<PT, FP, VL><<<gd, 32 * dwpc, dsm, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
-        b_run_g.as<uint64_t>(), b_dense_range.as<uint2>(), sc, (uint32_t)nd_cap,
-        b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
+        run_g, b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(), sc, (uint32_t)nd_cap,
+        b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c,
+        (uint32_t)k3all);
     CMH_LAUNCHED();
     k_befriend_simple<PT, FP, VL><<<gp, kT, 0, s>>>(
-        boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), b_run_g.as<uint64_t>(),
+        boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), run_g,
         sc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), queue, c);
     CMH_LAUNCHED();
     k_befriend<PT, FP, VL, 0><<<gw, kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
-        b_run_g.as<uint64_t>(), queue, sc, b_top_first.as<uint32_t>(),
+        run_g, queue, sc, b_top_first.as<uint32_t>(),
         b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
@@ -1464,7 +1556,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_LAUNCHED();
     k_befriend<PT, FP, VL, 1><<<gw, kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
-        b_run_g.as<uint64_t>(), queue, sc, b_top_first.as<uint32_t>(),
+        run_g, queue, sc, b_top_first.as<uint32_t>(),
         b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
@@ -1481,7 +1573,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaMemsetAsync(b_count.p, 0, npc * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_head.p, 0xff, npc * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_cand_of_root.p, 0xff, npc * 4, s));
-  k_group_count<<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
+  k_group_count<<<gp, kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
                                   b_vals.as<uint32_t>(), sc, b_count.as<uint32_t>(),
                                   b_head.as<uint32_t>());
   CMH_LAUNCHED();
@@ -1500,7 +1592,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, s));
   CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, (size_t)ncc * 4, s));
 #define CMH_SUMS(NSV)                                                                         \
-  k_group_sums<PT, NSV><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),  \
+  k_group_sums<PT, NSV><<<gp, kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),  \
                                           b_cand_of_root.as<uint32_t>(),                      \
                                           b_run_box.as<uint16_t>(), boxes,                    \
                                           b_spos.as<SPos<PT>>(), sc, props,                   \
@@ -1549,12 +1641,12 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_CUDA(cudaMemsetAsync(b_member.p, 0xff, (size_t)n * 8, s));
     CMH_CUDA(cudaMemsetAsync(b_member_proc.p, 0xff, (size_t)n * 4, s));
     CMH_CUDA(cudaMemsetAsync(b_member_pos.p, 0, (size_t)n * 12, s));
-    k_member<PT><<<gp, kT, 0, s>>>(b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(),
+    k_member<PT><<<gp, kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
                                    b_cand_of_root.as<uint32_t>(), b_cat_of_cand.as<uint32_t>(),
                                    b_spos.as<SPos<PT>>(), sc, b_member.as<unsigned long long>());
     CMH_LAUNCHED();
     k_member_copy<PT><<<gp, kT, 0, s>>>(
-        b_run_of.as<uint32_t>(), b_parent.as<uint32_t>(), b_cand_of_root.as<uint32_t>(),
+        run_of, b_parent.as<uint32_t>(), b_cand_of_root.as<uint32_t>(),
         b_cat_of_cand.as<uint32_t>(), b_run_box.as<uint16_t>(), boxd, nbox,
         b_spos.as<SPos<PT>>(), b_vals.as<uint32_t>(), sc, b_member.as<unsigned long long>(),
         b_member_proc.as<uint32_t>(), b_member_pos.as<float>(), c);
@@ -1616,7 +1708,10 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   // capacities: grown after a run that overflowed them, never shrunk
   const int64_t want_np = std::min<int64_t>(n_total + (int64_t)img, (int64_t)0xfffffff0ll);
   np_cap = std::max<int64_t>(np_cap, std::max<int64_t>(want_np, 1));
-  nd_cap = std::max<int64_t>(nd_cap, np_cap / 256 + 256);
+  // fine-cell maps of dense top cells: at most 8 bytes per processed
+  // particle plus 1 GiB (dense top cells past the cap are scanned instead)
+  nd_cap = std::max<int64_t>(nd_cap, np_cap / 1024 + 1024);
+  nd_cap = std::min<int64_t>(nd_cap, std::max<int64_t>(1024, maps_cap_for(np_cap, k3all)));
   double mincut = 1e300;
   for (const BoxDev &bd : boxes_host) mincut = std::min(mincut, bd.g.nphalomin);
   const int64_t div = (int64_t)std::max(1.0, std::floor(mincut));
@@ -1627,10 +1722,6 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   ctr.ensure(sizeof(Counters) + 2 * sizeof(unsigned long long));
   b_boxes.ensure(sizeof(BoxDev) * nbox);
   b_boxd.ensure(sizeof(uint32_t) * 7 * nbox);
-  b_keep.ensure(nn * 4);
-  b_nimg.ensure(nn * 4);
-  b_keep_scan.ensure(nn * 4);
-  b_img_scan.ensure(nn * 4);
   b_keys.ensure(npc * 8);
   b_keys_alt.ensure(npc * 8);
   b_vals.ensure(npc * 4);
@@ -1639,9 +1730,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   b_ppos.ensure(npc * rec);
   b_spos.ensure(npc * rec);
   if (varlink) b_svl.ensure(npc * sizeof(VLRec64));
-  b_run_of.ensure(npc * 4);
   b_run_start.ensure((npc + 1) * 4);
-  b_run_g.ensure(npc * 8);
   b_run_box.ensure(npc * 2);
   b_top_first.ensure(n_top * 4);
   b_top_end.ensure(n_top * 4);
@@ -1650,6 +1739,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   b_rtmp2.ensure(npc * 4);
   b_maps.ensure((size_t)nd_cap * k3all * 4);
   b_dense_range.ensure((size_t)nd_cap * sizeof(uint2));
+  b_dense_big.ensure((size_t)nd_cap * sizeof(uint32_t));
   b_parent.ensure(npc * 4);
   b_count.ensure(npc * 4);
   b_head.ensure(npc * 4);
@@ -1674,7 +1764,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   // shared memory of the dense-top kernel: one parent per fine cell of a top
   // cell (set here, outside any graph capture)
   {
-    const int dsm = (int)(k3all * sizeof(uint32_t));
+    const int dsm = (int)(dense_warps_per_cta(k3all) * k3all * sizeof(uint32_t));
     const void *dense[] = {
         (const void *)k_befriend_dense<float, true, false>,
         (const void *)k_befriend_dense<float, false, false>,
@@ -1765,6 +1855,10 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     const int64_t caps[6] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
                              (int64_t)dense_min};
     sig.insert(sig.end(), (const unsigned char *)caps, (const unsigned char *)caps + sizeof caps);
+    // and the workspace addresses the recorded launches use
+    each_buf([&](DevBuf &b) {
+      sig.insert(sig.end(), (const unsigned char *)&b.p, (const unsigned char *)&b.p + sizeof b.p);
+    });
     sig.insert(sig.end(), (const unsigned char *)ltab_all.data(),
                (const unsigned char *)(ltab_all.data() + ltab_all.size()));
     const bool same = graph_exec && sig == graph_sig;
@@ -1793,7 +1887,9 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
       if (!(last.overflow & 1u) && use_graph) capture(want_member, s, sig);
     }
     stats.n_launches = launches_per_run;
-    if (last.overflow & 2u) nd_cap = (int64_t)last.nd + last.nd / 4 + 256;  // faster next time
+    if (last.overflow & 2u)  // faster next time, within the map budget
+      nd_cap = std::min<int64_t>((int64_t)last.nd + last.nd / 4 + 256,
+                                 std::max<int64_t>(nd_cap, maps_cap_for(np_cap, k3all)));
     if (!(last.overflow & 1u)) return;
     np_cap = (int64_t)last.np_raw + last.np_raw / 8 + 4096;  // repeat with room
   }
@@ -1839,11 +1935,23 @@ cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaSt
     for (uint32_t dm : mins) {
       cell_scale = sc;
       dense_min = dm;
-      run_batch(specs, false, s);
+      // each setting starts from an empty workspace, so that one setting's
+      // large buffers (many top cells, or large maps) do not stay allocated
+      // under the next; a setting that does not fit in memory is skipped
+      release_workspace();
       float t = 0;
-      for (int r = 0; r < std::max(repeats, 1); r++) {
+      try {
         run_batch(specs, false, s);
-        t += stats.ms_total;
+        for (int r = 0; r < std::max(repeats, 1); r++) {
+          run_batch(specs, false, s);
+          t += stats.ms_total;
+        }
+      } catch (const Error &e) {
+        if (e.code != CMH_ERR_OUT_OF_MEMORY) {
+          use_graph = graph0;
+          throw;
+        }
+        continue;
       }
       t /= std::max(repeats, 1);
       best.tried++;
@@ -1853,9 +1961,11 @@ cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaSt
         best.dense_min = (int32_t)dm;
       }
     }
+  release_workspace();
+  use_graph = graph0;
+  if (best.tried == 0) fail(CMH_ERR_OUT_OF_MEMORY, "no setting of the autotuner fits in memory");
   cell_scale = best.cell_scale;
   dense_min = (uint32_t)best.dense_min;
-  use_graph = graph0;
   return best;
 }
 

@@ -71,7 +71,8 @@ struct DevScal {
   uint32_t R, nd, nc, nh;          // fine cells, dense top cells, candidates, halos
   uint32_t qcount, next_dense, next0, next1;
   uint32_t overflow;               // bit 0: processed particles above capacity
-  uint32_t pad[3];
+  uint32_t nbig, next_big;          // dense top cells handled by a whole CTA
+  uint32_t pad;
 };
 
 // Running counters of one run, in device memory.

@@ -59,14 +59,27 @@ struct Plan : public cmh_plan {
 
   // workspace
   DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
-  DevBuf b_keep, b_nimg, b_keep_scan, b_img_scan;
-  DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_svl, b_run_of;
-  DevBuf b_run_start, b_run_g, b_run_box, b_top_first, b_top_end, b_top_slot, b_rtmp1, b_rtmp2;
-  DevBuf b_maps, b_dense_range;
+  DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_svl;
+  DevBuf b_run_start, b_run_box, b_top_first, b_top_end, b_top_slot, b_rtmp1, b_rtmp2;
+  DevBuf b_maps, b_dense_range, b_dense_big;
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
   DevBuf in_pos, in_vel;  // device copies of host-resident particles
+
+  // every workspace buffer, for release and for the graph signature
+  template <class F> void each_buf(F f) {
+    DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd,
+                     &b_keys, &b_keys_alt, &b_vals, &b_vals_alt, &b_ppos, &b_spos, &b_svl,
+                     &b_run_start, &b_run_box, &b_top_first, &b_top_end, &b_top_slot,
+                     &b_rtmp1, &b_rtmp2, &b_maps, &b_dense_range, &b_dense_big, &b_parent, &b_count,
+                     &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
+                     &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
+                     &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
+                     &in_pos, &in_vel};
+    for (DevBuf *b : all) f(*b);
+  }
+  void release_workspace();
 
   Plan(const cmh_fof_params &p, int pos_dtype, int device);
   ~Plan() override;

@@ -215,3 +215,101 @@ def config5(seed=5, scale=1.0):
     w = make_box(n, L, round(500000 * n / 1024 ** 3), seed, nphalomin=20,
                  boundary=10.0, name="c5_box1024")
     return w
+
+
+def make_box_device(n, L, n_clumps, seed, *, device=0, linkb=0.2, nphalomin=10,
+                    boundary=10.0, clump_frac=0.6, name="box", chunk=1 << 26):
+    """make_box() drawn on a CUDA device with torch (same distributions, its
+    own random stream), for sizes whose host generation would take minutes:
+    positions float32, velocities float32, both torch tensors on `device`.
+    Clump members and background are drawn in chunks of `chunk` particles;
+    the array order is then a random permutation, as on the host."""
+    import torch
+
+    dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+    rng = np.random.default_rng(seed)
+    target = int(round(clump_frac * n))
+    n_clumps = max(int(n_clumps), 1)
+    counts, scale = _clump_masses(rng, n_clumps, target)
+    rs = 0.05 * np.cbrt(np.maximum(counts, 1) / 10.0)
+    centres = rng.random((n_clumps, 3)) * L
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+    cum = torch.from_numpy(np.cumsum(counts)).to(dev)
+    rs_t = torch.from_numpy(rs).to(dev)
+    cen_t = torch.from_numpy(centres).to(dev)
+    pos = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    Lf = torch.tensor(L, dtype=torch.float32).item()
+
+    def store(s, p):
+        p = torch.remainder(p, L).to(torch.float32)
+        p[p >= Lf] = 0.0                      # float rounding of L - tiny
+        pos[s:s + p.shape[0]] = p
+
+    for s in range(0, target, chunk):
+        e = min(s + chunk, target)
+        idx = torch.arange(s, e, device=dev)
+        cl = torch.searchsorted(cum, idx, right=True)
+        u = 0.999 * (1.0 - torch.rand(e - s, generator=g, device=dev, dtype=torch.float64))
+        r = rs_t[cl] / torch.sqrt(u ** (-2.0 / 3.0) - 1.0)
+        d = torch.randn((e - s, 3), generator=g, device=dev, dtype=torch.float64)
+        d /= torch.linalg.norm(d, dim=1, keepdim=True)
+        store(s, cen_t[cl] + d * r[:, None])
+        del idx, cl, u, r, d
+    for s in range(target, n, chunk):
+        e = min(s + chunk, n)
+        store(s, torch.rand((e - s, 3), generator=g, device=dev, dtype=torch.float64) * L)
+    perm = torch.randperm(n, generator=g, device=dev)
+    pos = pos[perm]
+    del perm
+    vel = torch.randn((n, 3), generator=g, device=dev, dtype=torch.float32) * SIGMA_V
+    torch.cuda.empty_cache()
+    sep = L / n ** (1.0 / 3.0)
+    return DeviceWorkload(name=name, pos=pos, vel=vel, lo=(0.0, 0.0, 0.0), hi=(float(L),) * 3,
+                          linklength=linkb * sep, boundary=float(boundary),
+                          nphalomin=float(nphalomin), periodic=True,
+                          cells=max(int(round(n ** (1.0 / 3.0))), 1),
+                          meta={"seed": seed, "n_clumps": n_clumps, "mass_scale": scale,
+                                "largest_clump": int(counts.max()), "mean_separation": sep,
+                                "linkb": linkb, "generated_on": str(dev)})
+
+
+@dataclass
+class DeviceWorkload:
+    """A Workload whose pos / vel are torch tensors on a CUDA device."""
+
+    name: str
+    pos: object
+    vel: object
+    lo: tuple
+    hi: tuple
+    linklength: float
+    boundary: float
+    nphalomin: float
+    periodic: bool
+    cells: int
+    varlink: dict | None = None
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    def to_host(self) -> Workload:
+        """The same particles as a host Workload (for checks at small sizes)."""
+        import numpy as _np
+        pos = self.pos.cpu().numpy()
+        return Workload(name=self.name, pos=pos, vel=self.vel.cpu().numpy(),
+                        ids=_np.arange(pos.shape[0], dtype=_np.uint64), lo=self.lo,
+                        hi=self.hi, linklength=self.linklength, boundary=self.boundary,
+                        nphalomin=self.nphalomin, periodic=self.periodic, cells=self.cells,
+                        varlink=self.varlink, meta=dict(self.meta))
+
+
+def config5_device(seed=5, scale=1.0, device=0):
+    """config5 at full size (1024^3 = 1.07e9 particles, 25.8 GB of float32
+    positions and velocities) generated on the device."""
+    n = max(int(round(1024 ** 3 * scale)), 64)
+    L = 2000.0 * (n / 1024 ** 3) ** (1.0 / 3.0)
+    return make_box_device(n, L, round(500000 * n / 1024 ** 3), seed, device=device,
+                           nphalomin=20, boundary=10.0, name="c5_box1024")

@@ -200,6 +200,10 @@ cmh_status cmh_plan_autotune(cmh_plan *plan, const cmh_fof_params *params,
                              const cmh_particles *parts, int32_t nbox, int32_t repeats,
                              void *stream, cmh_tuning *out);
 
+/* Applies a setting found earlier (cell_scale > 0, dense_min >= 1) to a
+ * plan without timing anything; ms and tried are ignored. */
+cmh_status cmh_plan_set_tuning(cmh_plan *plan, const cmh_tuning *tuning);
+
 /* cmh_fof_run_batch on a plan: repeated batches of the same shape replay one
  * CUDA graph. */
 cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,

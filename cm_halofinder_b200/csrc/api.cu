@@ -1,12 +1,16 @@
 // C ABI of the FoF library (include/cmh_fof.h): plans, one-shot runs,
 // catalogs, errors.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 
 #include "cmh_internal.cuh"
 #include "plan.cuh"
@@ -33,6 +37,23 @@ void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
 }
 
 void fail(cmh_status code, const std::string &msg) { throw Error{code, msg}; }
+
+int resident_ctas(const void *kernel, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void *, int, size_t, int>, int> cache;
+  int dev = 0, sms = kSMs;
+  CMH_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(kernel, threads, smem, dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0;
+  CMH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  CMH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int n = std::max(1, per_sm) * std::max(1, sms);
+  cache[key] = n;
+  return n;
+}
 
 void DevBuf::ensure(size_t bytes) {
   if (bytes <= cap && p) return;

@@ -42,6 +42,19 @@ inline unsigned grid_for(int64_t n, int threads, int per_sm = 8) {
   return (unsigned)(want < cap ? want : cap);
 }
 
+// CTAs of `kernel` (with `threads` threads and `smem` bytes of dynamic shared
+// memory) resident at once on the current device: per-SM occupancy times the
+// SM count, cached per kernel, shape and device.
+int resident_ctas(const void *kernel, int threads, size_t smem);
+
+// Grid for a grid-stride kernel: one resident wave, capped by the work.
+inline unsigned grid_resident(const void *kernel, int threads, size_t smem, int64_t n) {
+  int64_t want = (n + threads - 1) / threads;
+  const int64_t cap = resident_ctas(kernel, threads, smem);
+  if (want < 1) want = 1;
+  return (unsigned)(want < cap ? want : cap);
+}
+
 // Growable device buffer.
 struct DevBuf {
   void *p = nullptr;

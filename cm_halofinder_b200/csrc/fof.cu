@@ -181,7 +181,7 @@ __device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint6
 #pragma unroll
   for (int a = 0; a < 3; a++) gi[a] = fine_index(c[a], g.rmin[a], g.inv_h, g.G[a]);
   const int k = g.k;
-  const int t[3] = {gi[0] / k, gi[1] / k, gi[2] / k};
+  const int t[3] = {div_k(gi[0], g), div_k(gi[1], g), div_k(gi[2], g)};
   const uint64_t top = top_base + ((uint64_t)t[2] * g.T[1] + t[1]) * g.T[0] + t[0];
   const uint64_t sub = ((uint64_t)(gi[2] - t[2] * k) * k + (gi[1] - t[1] * k)) * k + (gi[0] - t[0] * k);
   keys[p] = top * k3all + sub;
@@ -351,23 +351,22 @@ __global__ void __launch_bounds__(kT) k_varlink_recs(const SPos<PT> *__restrict_
 
 __device__ __forceinline__ uint64_t top_of_run(const BoxDev &bx, uint64_t pg) {
   const Geom &g = bx.g;
-  const int k = g.k;
-  const uint64_t gx = pg & kM21, gy = (pg >> 21) & kM21, gz = pg >> 42;
-  return bx.top_base + ((gz / k) * g.T[1] + gy / k) * g.T[0] + gx / k;
+  const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
+  return bx.top_base +
+         ((uint64_t)div_k(gz, g) * g.T[1] + (uint64_t)div_k(gy, g)) * g.T[0] + div_k(gx, g);
 }
 
 __global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ run_g,
                                                    const uint16_t *__restrict__ run_box,
                                                    const BoxDev *__restrict__ boxes,
                                                    const DevScal *__restrict__ sc,
-                                                   uint32_t *__restrict__ top_first,
-                                                   uint32_t *__restrict__ top_end) {
+                                                   uint32_t *__restrict__ top_range) {
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
     const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
-    if (r == 0 || top_of_run(boxes[run_box[r - 1]], run_g[r - 1]) != t) top_first[t] = (uint32_t)r;
+    if (r == 0 || top_of_run(boxes[run_box[r - 1]], run_g[r - 1]) != t) top_range[2 * t] = (uint32_t)r;
     if (r == R - 1 || top_of_run(boxes[run_box[r + 1]], run_g[r + 1]) != t)
-      top_end[t] = (uint32_t)(r + 1);
+      top_range[2 * t + 1] = (uint32_t)(r + 1);
   }
 }
 
@@ -377,8 +376,7 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
                                                     const uint16_t *__restrict__ run_box,
                                                     const BoxDev *__restrict__ boxes,
                                                     const DevScal *__restrict__ sc, int64_t cap,
-                                                    const uint32_t *__restrict__ top_first,
-                                                    const uint32_t *__restrict__ top_end,
+                                                    const uint2 *__restrict__ top_range,
                                                     uint32_t dense_min,
                                                     uint32_t *__restrict__ flag) {
   const uint32_t R = sc->R;
@@ -386,7 +384,8 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
     uint32_t f = 0;
     if (r < R) {
       const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
-      f = (top_first[t] == (uint32_t)r && top_end[t] - top_first[t] > dense_min) ? 1u : 0u;
+      const uint2 tr = top_range[t];
+      f = (tr.x == (uint32_t)r && tr.y - tr.x > dense_min) ? 1u : 0u;
     }
     flag[r] = f;
   }
@@ -403,8 +402,7 @@ __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ 
                                                    const uint16_t *__restrict__ run_box,
                                                    const BoxDev *__restrict__ boxes,
                                                    DevScal *sc, uint64_t k3all,
-                                                   const uint32_t *__restrict__ top_first,
-                                                   const uint32_t *__restrict__ top_end,
+                                                   const uint2 *__restrict__ top_range,
                                                    const uint32_t *__restrict__ dflag,
                                                    const uint32_t *__restrict__ dscan,
                                                    uint32_t dense_min, uint32_t nd_cap,
@@ -417,18 +415,20 @@ __global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ 
     const BoxDev &bx = boxes[run_box[r]];
     const uint64_t pg = run_g[r];
     const uint64_t t = top_of_run(bx, pg);
-    const uint32_t f = top_first[t];
-    if (top_end[t] - f <= dense_min) continue;
+    const uint2 tr = top_range[t];
+    const uint32_t f = tr.x;
+    if (tr.y - f <= dense_min) continue;
     const uint32_t slot = dscan[f];  // the first fine cell of the top cell carries the slot
     if (slot >= nd_cap) continue;
     if (dflag[r]) {
       top_slot[t] = slot;
-      dense_range[slot] = make_uint2(f, top_end[t]);
-      if (top_end[t] - f > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
+      dense_range[slot] = tr;
+      if (tr.y - f > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
     }
     const int k = bx.g.k;
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-    const uint64_t sub = ((uint64_t)(gz % k) * k + (gy % k)) * k + (gx % k);
+    const uint64_t sub = ((uint64_t)(gz - div_k(gz, bx.g) * k) * k + (gy - div_k(gy, bx.g) * k)) * k +
+                         (gx - div_k(gx, bx.g) * k);
     maps[(uint64_t)slot * k3all + sub] = (int32_t)r;
   }
 }
@@ -657,7 +657,7 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
       const uint32_t a = f + i;
       const uint64_t pg = run_g[a];
       const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-      const int sx = gx % k, sy = gy % k, sz = gz % k;
+      const int sx = gx - div_k(gx, g) * k, sy = gy - div_k(gy, g) * k, sz = gz - div_k(gz, g) * k;
       const uint32_t sa = run_start[a], ea = run_start[a + 1];
       for (int dz = 0; dz <= W; dz++)
         for (int dy = -W; dy <= W; dy++)
@@ -753,26 +753,37 @@ __device__ __forceinline__ bool reaches(int s, int o, int k, int W) {
 // and the cell is finished in two L2 round trips.  Other cells are queued for
 // the warp path below.
 constexpr uint32_t kSimple = 2;  // two slot bits per range below
+constexpr uint32_t kSimpleChunk = 1024;  // fine cells per grab of a CTA
 
 template <class PT, bool FP32, bool VL>
 __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g, DevScal *sc,
-    const uint32_t *__restrict__ top_first, const uint32_t *__restrict__ top_end,
+    const uint2 *__restrict__ top_range,
     const uint32_t *__restrict__ top_slot, const SPos<PT> *__restrict__ spos,
     const VLRec<FP32> *__restrict__ svl, uint32_t *parent, uint32_t *__restrict__ queue,
     Counters *ctr) {
   const uint32_t R = sc->R;
   const int lane = threadIdx.x & 31;
+  __shared__ uint32_t s_base;
   BfStats st;
-  for (int64_t ai = gtid(); ai < R; ai += gstride()) {
-    const uint32_t a = (uint32_t)ai;
+  // CTAs take chunks of consecutive fine cells from a counter: the work per
+  // cell varies a lot across the box (clumps, queued cells), and a static
+  // share would leave the CTAs of the busy regions running alone at the end
+  while (true) {
+    if (threadIdx.x == 0) s_base = atomicAdd(&sc->next_simple, kSimpleChunk);
+    __syncthreads();
+    const uint32_t base = s_base;
+    __syncthreads();
+    if (base >= R) break;
+    const uint32_t end = min(base + kSimpleChunk, R);
+    for (uint32_t a = base + threadIdx.x; a < end; a += blockDim.x) {
     const BoxDev &bx = boxes[run_box[a]];
     const Geom &g = bx.g;
     const int k = g.k, W = g.W;
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-    const int tx = gx / k, ty = gy / k, tz = gz / k;
+    const int tx = div_k(gx, g), ty = div_k(gy, g), tz = div_k(gz, g);
     const int sx = gx - tx * k, sy = gy - ty * k, sz = gz - tz * k;
     uint32_t R0[14], NN[14];
 #pragma unroll
@@ -783,7 +794,8 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
                       reaches(sx, kFwd[nb][0], k, W) && reaches(sy, kFwd[nb][1], k, W) &&
                       reaches(sz, kFwd[nb][2], k, W);
       const uint64_t tb = in ? bx.top_base + ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux : 0;
-      const uint32_t f = in ? top_first[tb] : 0u, e = in ? top_end[tb] : 0u;
+      const uint2 tr = in ? top_range[tb] : make_uint2(0u, 0u);
+      const uint32_t f = tr.x, e = tr.y;
       R0[nb] = nb == 0 ? a + 1 : f;
       NN[nb] = e > R0[nb] ? e - R0[nb] : 0u;
       // pairs inside a dense top cell are joined by k_befriend_dense
@@ -836,6 +848,7 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
       try_link<PT, FP32, VL>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent,
                              ctr, st);
     }
+    }
   }
   st.flush(ctr);
 }
@@ -853,8 +866,8 @@ template <class PT, bool FP32, bool VL, int PHASE>
 __global__ void __launch_bounds__(kT) k_befriend(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
-    const uint32_t *__restrict__ queue, DevScal *sc, const uint32_t *__restrict__ top_first,
-    const uint32_t *__restrict__ top_end, const uint32_t *__restrict__ top_slot,
+    const uint32_t *__restrict__ queue, DevScal *sc, const uint2 *__restrict__ top_range,
+    const uint32_t *__restrict__ top_slot,
     const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
     const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr) {
   const uint32_t NQ = sc->qcount;
@@ -872,7 +885,7 @@ __global__ void __launch_bounds__(kT) k_befriend(
     const int k = g.k, W = g.W;
     const uint64_t pg = run_g[a];
     const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-    const int tx = gx / k, ty = gy / k, tz = gz / k;
+    const int tx = div_k(gx, g), ty = div_k(gy, g), tz = div_k(gz, g);
     const uint32_t sa = run_start[a], ea = run_start[a + 1];
     uint32_t ra = __ldcg(parent + a);
     const int sx = gx - tx * k, sy = gy - ty * k, sz = gz - tz * k;
@@ -885,7 +898,8 @@ __global__ void __launch_bounds__(kT) k_befriend(
           reaches(sx, kFwd[lane][0], k, W) && reaches(sy, kFwd[lane][1], k, W) &&
           reaches(sz, kFwd[lane][2], k, W)) {
         const uint64_t tb = bx.top_base + ((uint64_t)uz * g.T[1] + uy) * g.T[0] + ux;
-        const uint32_t f = top_first[tb], e = top_end[tb];
+        const uint2 tr = top_range[tb];
+        const uint32_t f = tr.x, e = tr.y;
         const uint32_t slot = top_slot[tb];
         r0 = lane == 0 ? a + 1 : f;
         // pairs inside a mapped top cell are joined by k_befriend_dense
@@ -1395,6 +1409,7 @@ Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &lta
       if (T >= (1ull << 31)) fail(CMH_ERR_CAPACITY, "domain too large for the top-cell grid");
       g.k = k;
       g.k3 = (uint64_t)k * k * k;
+      g.kmul = (uint32_t)((1ull << 32) / (uint64_t)k + 1);
       break;
     }
     k++;
@@ -1403,6 +1418,12 @@ Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &lta
 }
 
 namespace {
+// Grid of a grid-stride kernel of kT threads: the CTAs that can be resident
+// at once, capped by the work.
+template <class K> unsigned rg(K *kernel, int64_t n) {
+  return grid_resident(reinterpret_cast<const void *>(kernel), kT, 0, n);
+}
+
 // Warps per CTA of the dense-top kernel: up to 4, each with k^3 parents of
 // shared memory, within 200 KiB per CTA.
 int dense_warps_per_cta(uint64_t k3all) {
@@ -1452,7 +1473,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 
   // ---- ingest ----
   if (n > 0) {
-    k_ingest_count<PT><<<grid_for(n, kT), kT, 0, s>>>(boxes, nbox, n, keep,
+    k_ingest_count<PT><<<rg(k_ingest_count<PT>, n), kT, 0, s>>>(boxes, nbox, n, keep,
                                                       nimg);
     CMH_LAUNCHED();
   }
@@ -1464,7 +1485,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                 img_scan, sc, boxd, (uint32_t)npc);
   CMH_LAUNCHED();
   if (n > 0) {
-    k_ingest_emit<PT><<<grid_for(n, kT), kT, 0, s>>>(
+    k_ingest_emit<PT><<<rg(k_ingest_emit<PT>, n), kT, 0, s>>>(
         boxes, nbox, n, k3all, keep, keep_scan,
         img_scan, nimg, boxd, (uint32_t)npc,
         b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
@@ -1478,55 +1499,52 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   // ---- runs, top-cell ranges, dense maps ----
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
   uint32_t *run_scan = flag + npc;
-  const unsigned gp = grid_for(npc, kT);
-  k_gather_flags<PT><<<gp, kT, 0, s>>>(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(),
+  k_gather_flags<PT><<<rg(k_gather_flags<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(),
                                        b_ppos.as<SPos<PT>>(), b_spos.as<SPos<PT>>(), flag, sc,
                                        npc);
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s);
-  k_runs<<<gp, kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, boxes, nbox, k3all, sc,
+  k_runs<<<rg(k_runs, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, boxes, nbox, k3all, sc,
                            run_of, b_run_start.as<uint32_t>(),
                            run_g, b_run_box.as<uint16_t>());
   CMH_LAUNCHED();
   if (varlink) {
     if (fp32)
-      k_varlink_recs<PT, true><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
+      k_varlink_recs<PT, true><<<rg(k_varlink_recs<PT, true>, npc), kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
                                                  b_run_box.as<uint16_t>(), boxes, sc,
                                                  b_svl.as<VLRec32>());
     else
-      k_varlink_recs<PT, false><<<gp, kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
+      k_varlink_recs<PT, false><<<rg(k_varlink_recs<PT, false>, npc), kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
                                                   b_run_box.as<uint16_t>(), boxes, sc,
                                                   b_svl.as<VLRec64>());
     CMH_LAUNCHED();
   }
-  CMH_CUDA(cudaMemsetAsync(b_top_first.p, 0, n_top * 4, s));
-  CMH_CUDA(cudaMemsetAsync(b_top_end.p, 0, n_top * 4, s));
+  CMH_CUDA(cudaMemsetAsync(b_top_range.p, 0, n_top * 8, s));
   CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, s));
-  k_top_ranges<<<gp, kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                 b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>());
+  k_top_ranges<<<rg(k_top_ranges, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
+                                 b_top_range.as<uint32_t>());
   CMH_LAUNCHED();
-  k_dense_flags<<<gp, kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                  npc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(),
+  k_dense_flags<<<rg(k_dense_flags, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
+                                  npc, b_top_range.as<uint2>(),
                                   dense_min, b_rtmp1.as<uint32_t>());
   CMH_LAUNCHED();
   exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s);
   k_clamp_dense<<<1, 32, 0, s>>>(sc, (uint32_t)nd_cap);
   CMH_LAUNCHED();
   CMH_CUDA(cudaMemsetAsync(b_maps.p, 0xff, (size_t)nd_cap * k3all * 4, s));
-  k_dense_maps<<<gp, kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                 k3all, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(),
+  k_dense_maps<<<rg(k_dense_maps, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
+                                 k3all, b_top_range.as<uint2>(),
                                  b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), dense_min,
                                  (uint32_t)nd_cap, b_top_slot.as<uint32_t>(),
                                  b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(),
                                  b_maps.as<int32_t>());
   CMH_LAUNCHED();
-  k_iota<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
+  k_iota<<<rg(k_iota, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
   mark(2);
   // ---- befriending: dense top cells inside (CTA each), fast path, queue,
   // warp path near then far ----
   uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
-  const unsigned gw = grid_for(npc * 32, kT);
   const int dwpc = dense_warps_per_cta(k3all);
   const size_t dsm = (size_t)dwpc * k3all * sizeof(uint32_t);
   const unsigned gd = (unsigned)std::max<int64_t>(
@@ -1541,23 +1559,23 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
         b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c,
         (uint32_t)k3all);
     CMH_LAUNCHED();
-    k_befriend_simple<PT, FP, VL><<<gp, kT, 0, s>>>(
+    k_befriend_simple<PT, FP, VL><<<rg(k_befriend_simple<PT, FP, VL>, npc), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), run_g,
-        sc, b_top_first.as<uint32_t>(), b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(),
+        sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), queue, c);
     CMH_LAUNCHED();
-    k_befriend<PT, FP, VL, 0><<<gw, kT, 0, s>>>(
+    k_befriend<PT, FP, VL, 0><<<rg(k_befriend<PT, FP, VL, 0>, npc * 32), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
-        run_g, queue, sc, b_top_first.as<uint32_t>(),
-        b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
+        run_g, queue, sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
+        b_maps.as<int32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
-    k_compress<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
+    k_compress<<<rg(k_compress, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
     CMH_LAUNCHED();
-    k_befriend<PT, FP, VL, 1><<<gw, kT, 0, s>>>(
+    k_befriend<PT, FP, VL, 1><<<rg(k_befriend<PT, FP, VL, 1>, npc * 32), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
-        run_g, queue, sc, b_top_first.as<uint32_t>(),
-        b_top_end.as<uint32_t>(), b_top_slot.as<uint32_t>(), b_maps.as<int32_t>(),
+        run_g, queue, sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
+        b_maps.as<int32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
   };
@@ -1565,7 +1583,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   else if (fp32) befriend(std::true_type{}, std::false_type{});
   else if (varlink) befriend(std::false_type{}, std::true_type{});
   else befriend(std::false_type{}, std::false_type{});
-  k_compress<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
+  k_compress<<<rg(k_compress, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
   mark(3);
 
@@ -1573,16 +1591,16 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaMemsetAsync(b_count.p, 0, npc * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_head.p, 0xff, npc * 4, s));
   CMH_CUDA(cudaMemsetAsync(b_cand_of_root.p, 0xff, npc * 4, s));
-  k_group_count<<<gp, kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
+  k_group_count<<<rg(k_group_count, npc), kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
                                   b_vals.as<uint32_t>(), sc, b_count.as<uint32_t>(),
                                   b_head.as<uint32_t>());
   CMH_LAUNCHED();
-  k_cand_flags<<<gp, kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(),
+  k_cand_flags<<<rg(k_cand_flags, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(),
                                  b_run_box.as<uint16_t>(), boxes, sc, npc,
                                  b_rtmp1.as<uint32_t>(), extra + 0);
   CMH_LAUNCHED();
   exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nc, scan_tmp, s);
-  k_cand_list<<<gp, kT, 0, s>>>(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), sc,
+  k_cand_list<<<rg(k_cand_list, npc), kT, 0, s>>>(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), sc,
                                 b_cand_of_root.as<uint32_t>(), b_cand_root.as<uint32_t>());
   CMH_LAUNCHED();
   mark(4);
@@ -1592,7 +1610,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, s));
   CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, (size_t)ncc * 4, s));
 #define CMH_SUMS(NSV)                                                                         \
-  k_group_sums<PT, NSV><<<gp, kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),  \
+  k_group_sums<PT, NSV><<<rg(k_group_sums<PT, NSV>, npc), kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),  \
                                           b_cand_of_root.as<uint32_t>(),                      \
                                           b_run_box.as<uint16_t>(), boxes,                    \
                                           b_spos.as<SPos<PT>>(), sc, props,                   \
@@ -1603,9 +1621,8 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 #undef CMH_SUMS
   CMH_LAUNCHED();
   mark(5);
-  const unsigned gc = grid_for(ncc, kT);
 #define CMH_OWNED(NSV)                                                                          \
-  k_owned<NSV><<<gc, kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),              \
+  k_owned<NSV><<<rg(k_owned<NSV>, ncc), kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),              \
                                  b_count.as<uint32_t>(), b_run_box.as<uint16_t>(), boxes, sc, \
                                  ncc, b_own.as<uint32_t>())
   if (NS == 6) CMH_OWNED(6);
@@ -1614,7 +1631,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 #undef CMH_OWNED
   CMH_LAUNCHED();
   exclusive_scan_u32(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(), ncc, &sc->nh, scan_tmp, s);
-  k_own_list<<<gc, kT, 0, s>>>(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(),
+  k_own_list<<<rg(k_own_list, ncc), kT, 0, s>>>(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(),
                                b_cand_root.as<uint32_t>(), b_head.as<uint32_t>(), sc,
                                b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>());
   CMH_LAUNCHED();
@@ -1623,7 +1640,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                      sort_tmp, scan_tmp, s);
   CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, (size_t)ncc * 4, s));
 #define CMH_CATALOG(NSV)                                                                        \
-  k_catalog<NSV><<<gc, kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc,          \
+  k_catalog<NSV><<<rg(k_catalog<NSV>, ncc), kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc,          \
                                    b_sums.as<double>(), b_cand_root.as<uint32_t>(),             \
                                    b_count.as<uint32_t>(), b_warn.as<uint32_t>(),               \
                                    b_run_box.as<uint16_t>(), boxd, nbox, props, hs,              \
@@ -1641,11 +1658,11 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_CUDA(cudaMemsetAsync(b_member.p, 0xff, (size_t)n * 8, s));
     CMH_CUDA(cudaMemsetAsync(b_member_proc.p, 0xff, (size_t)n * 4, s));
     CMH_CUDA(cudaMemsetAsync(b_member_pos.p, 0, (size_t)n * 12, s));
-    k_member<PT><<<gp, kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
+    k_member<PT><<<rg(k_member<PT>, npc), kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
                                    b_cand_of_root.as<uint32_t>(), b_cat_of_cand.as<uint32_t>(),
                                    b_spos.as<SPos<PT>>(), sc, b_member.as<unsigned long long>());
     CMH_LAUNCHED();
-    k_member_copy<PT><<<gp, kT, 0, s>>>(
+    k_member_copy<PT><<<rg(k_member_copy<PT>, npc), kT, 0, s>>>(
         run_of, b_parent.as<uint32_t>(), b_cand_of_root.as<uint32_t>(),
         b_cat_of_cand.as<uint32_t>(), b_run_box.as<uint16_t>(), boxd, nbox,
         b_spos.as<SPos<PT>>(), b_vals.as<uint32_t>(), sc, b_member.as<unsigned long long>(),
@@ -1732,8 +1749,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   if (varlink) b_svl.ensure(npc * sizeof(VLRec64));
   b_run_start.ensure((npc + 1) * 4);
   b_run_box.ensure(npc * 2);
-  b_top_first.ensure(n_top * 4);
-  b_top_end.ensure(n_top * 4);
+  b_top_range.ensure(n_top * 8);
   b_top_slot.ensure(n_top * 4);
   b_rtmp1.ensure(npc * 4);
   b_rtmp2.ensure(npc * 4);

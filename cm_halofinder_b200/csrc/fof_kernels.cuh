@@ -40,6 +40,7 @@ struct Geom {
   int G[3];              // fine cells per axis
   int T[3];              // top cells per axis
   uint64_t k3;           // k^3
+  uint32_t kmul;         // floor(2^32 / k) + 1: x / k == umulhi(x, kmul) for x < 2^27
   int props;             // CMH_PROP_* bits
   int hs;                // floats per halo record
   // variable linking length
@@ -72,7 +73,7 @@ struct DevScal {
   uint32_t qcount, next_dense, next0, next1;
   uint32_t overflow;               // bit 0: processed particles above capacity
   uint32_t nbig, next_big;          // dense top cells handled by a whole CTA
-  uint32_t pad;
+  uint32_t next_simple;             // fine cells taken by the sparse path
 };
 
 // Running counters of one run, in device memory.
@@ -180,6 +181,13 @@ __device__ __forceinline__ bool ref_neighbours(uint64_t a, uint64_t b) {
     ok &= d >= -1 && d <= 1;
   }
   return ok;
+}
+
+// x / k for a fine-cell coordinate x < 2^21 (2 <= k <= 32): with kmul =
+// floor(2^32 / k) + 1 = (2^32 + e) / k, 0 < e <= k, x kmul / 2^32 = x / k +
+// x e / (k 2^32), and the second term stays below 1/k, so the floor is exact.
+__device__ __forceinline__ int div_k(int x, const Geom &g) {
+  return (int)__umulhi((uint32_t)x, g.kmul);
 }
 
 // Fine-cell index along one axis: floor((x - rmin) * (1/h)), in double.  Two

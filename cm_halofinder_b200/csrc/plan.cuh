@@ -60,7 +60,7 @@ struct Plan : public cmh_plan {
   // workspace
   DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
   DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_svl;
-  DevBuf b_run_start, b_run_box, b_top_first, b_top_end, b_top_slot, b_rtmp1, b_rtmp2;
+  DevBuf b_run_start, b_run_box, b_top_range, b_top_slot, b_rtmp1, b_rtmp2;
   DevBuf b_maps, b_dense_range, b_dense_big;
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
@@ -71,7 +71,7 @@ struct Plan : public cmh_plan {
   template <class F> void each_buf(F f) {
     DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd,
                      &b_keys, &b_keys_alt, &b_vals, &b_vals_alt, &b_ppos, &b_spos, &b_svl,
-                     &b_run_start, &b_run_box, &b_top_first, &b_top_end, &b_top_slot,
+                     &b_run_start, &b_run_box, &b_top_range, &b_top_slot,
                      &b_rtmp1, &b_rtmp2, &b_maps, &b_dense_range, &b_dense_big, &b_parent, &b_count,
                      &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
                      &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,

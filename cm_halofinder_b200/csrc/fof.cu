@@ -631,12 +631,20 @@ __device__ __forceinline__ void lunion(uint32_t *lp, uint32_t a, uint32_t b, Cou
   atomicAdd(&ctr->uf_giveups, 1u);
 }
 
+// Bits lo..hi (0 <= lo <= hi <= 31) set.
+__device__ __forceinline__ uint32_t bit_span(int lo, int hi) {
+  return (hi - lo == 31 ? 0xffffffffu : ((1u << (hi - lo + 1)) - 1u)) << lo;
+}
+
 // Dense top cells: the fine-cell pairs inside a top cell are joined with a
-// union-find in shared memory (neighbours found through the top cell's
-// fine-cell map), near pairs before far ones; then every fine cell's global
-// parent is set to its local root.  Links that cross the top cell's faces
-// are left to the global passes.  `tid`/`nt` number the threads that share
-// the top cell and `sync` is their barrier.
+// union-find in shared memory, near pairs before far ones; then every fine
+// cell's global parent is set to its local root.  Links that cross the top
+// cell's faces are left to the global passes.  The occupied fine cells of
+// the top cell are first marked in bit rows (bit x of rows[z k + y]), so a
+// cell visits only the occupied cells of its forward window, a row at a
+// time, and reads the fine-cell map only for those.  `tid`/`nt` number the
+// threads that share the top cell and `sync` is their barrier; `lpar` holds
+// k3all parents followed by the k^2 rows.
 template <class PT, bool FP32, bool VL, class Sync>
 __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_t tid,
                                           uint32_t nt, Sync sync, const BoxDev *boxes,
@@ -649,7 +657,16 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
   const uint32_t f = fr.x, n = fr.y - fr.x;
   const Geom &g = boxes[run_box[f]].g;
   const int k = g.k, W = g.W;
+  uint32_t *rows = lpar + k3all;
   for (uint32_t i = tid; i < n; i += nt) lpar[i] = i;
+  for (uint32_t j = tid; j < (uint32_t)(k * k); j += nt) rows[j] = 0u;
+  sync();
+  for (uint32_t i = tid; i < n; i += nt) {
+    const uint64_t pg = run_g[f + i];
+    const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
+    atomicOr(rows + (gz - div_k(gz, g) * k) * k + (gy - div_k(gy, g) * k),
+             1u << (gx - div_k(gx, g) * k));
+  }
   sync();
   const int32_t *map = maps + (uint64_t)slot * k3all;
   for (int pass = 0; pass < 2; pass++) {
@@ -659,14 +676,24 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
       const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
       const int sx = gx - div_k(gx, g) * k, sy = gy - div_k(gy, g) * k, sz = gz - div_k(gz, g) * k;
       const uint32_t sa = run_start[a], ea = run_start[a + 1];
-      for (int dz = 0; dz <= W; dz++)
-        for (int dy = -W; dy <= W; dy++)
-          for (int dx = -W; dx <= W; dx++) {
-            if (dz == 0 && (dy < 0 || (dy == 0 && dx <= 0))) continue;  // forward only
-            const int cheb = max(abs(dx), max(abs(dy), dz));
-            if ((pass == 0) != (cheb <= 1)) continue;
-            const int tx = sx + dx, ty = sy + dy, tz = sz + dz;
-            if (tx < 0 || ty < 0 || tx >= k || ty >= k || tz >= k) continue;
+      // columns within reach, and the near ones (|dx| <= 1)
+      const uint32_t reach = bit_span(max(sx - W, 0), min(sx + W, k - 1));
+      const uint32_t near = bit_span(max(sx - 1, 0), min(sx + 1, k - 1));
+      const uint32_t after = sx == 31 ? 0u : (0xffffffffu << (sx + 1));
+      for (int dz = 0; dz <= W && sz + dz < k; dz++)
+        for (int dy = (dz == 0 ? 0 : -W); dy <= W; dy++) {
+          const int ty = sy + dy;
+          if (ty < 0 || ty >= k) continue;
+          const int rc = max(abs(dy), dz);  // the row's distance in y and z
+          uint32_t m;
+          if (pass == 0) m = rc <= 1 ? near : 0u;       // Chebyshev distance <= 1
+          else m = rc <= 1 ? (reach & ~near) : reach;   // Chebyshev distance >= 2
+          if (dz == 0 && dy == 0) m &= after;           // forward only in a's own row
+          const int tz = sz + dz;
+          uint32_t bits = rows[tz * k + ty] & m;
+          while (bits) {
+            const int tx = __ffs(bits) - 1;
+            bits &= bits - 1u;
             const int32_t r = map[(tz * k + ty) * k + tx];
             if (r < 0) continue;
             st.cand++;
@@ -677,12 +704,13 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
               continue;
             }
             auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
-            if (cells_linked<PT, FP32, VL>(g, (uint32_t)r, gx + dx, gy + dy, gz + dz, sa, ea,
-                                           run_start, spos, svl, st, apart)) {
+            if (cells_linked<PT, FP32, VL>(g, (uint32_t)r, gx + (tx - sx), gy + dy, gz + dz, sa,
+                                           ea, run_start, spos, svl, st, apart)) {
               lunion(lpar, ri, rj, ctr);
               st.unions++;
             }
           }
+        }
     }
     sync();
   }
@@ -693,8 +721,8 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
 // The dense top cells.  The big ones (more than kBigTop fine cells, listed
 // in `big`) go first, one per CTA, so that the largest, which bound the
 // kernel's length, start early and have many threads; then each warp takes
-// the small ones one at a time, with its own slice of `lstride` parents of
-// shared memory.  Both kinds are taken from atomic counters: their sizes
+// the small ones one at a time, with its own slice of `lstride` words of
+// shared memory (parents and bit rows).  Both kinds are taken from atomic counters: their sizes
 // differ widely.
 template <class PT, bool FP32, bool VL>
 __global__ void __launch_bounds__(128) k_befriend_dense(
@@ -863,7 +891,7 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
 // neighbourhood is joined (and compressed) before its far pairs are tried and
 // most of those become root skips.
 template <class PT, bool FP32, bool VL, int PHASE>
-__global__ void __launch_bounds__(kT) k_befriend(
+__global__ void __launch_bounds__(kT, 4) k_befriend(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint32_t *__restrict__ queue, DevScal *sc, const uint2 *__restrict__ top_range,
@@ -1424,10 +1452,16 @@ template <class K> unsigned rg(K *kernel, int64_t n) {
   return grid_resident(reinterpret_cast<const void *>(kernel), kT, 0, n);
 }
 
-// Warps per CTA of the dense-top kernel: up to 4, each with k^3 parents of
-// shared memory, within 200 KiB per CTA.
+// Shared-memory words of one dense top cell: k^3 parents and k^2 bit rows.
+uint64_t dense_words(uint64_t k3all) {
+  const uint64_t k = (uint64_t)std::llround(std::cbrt((double)k3all));
+  return k3all + k * k;
+}
+
+// Warps per CTA of the dense-top kernel: up to 4, each with the words of one
+// top cell, within 200 KiB per CTA.
 int dense_warps_per_cta(uint64_t k3all) {
-  const uint64_t per = k3all * sizeof(uint32_t);
+  const uint64_t per = dense_words(k3all) * sizeof(uint32_t);
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(4, (200u << 10) / per));
 }
 
@@ -1546,7 +1580,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   // warp path near then far ----
   uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
   const int dwpc = dense_warps_per_cta(k3all);
-  const size_t dsm = (size_t)dwpc * k3all * sizeof(uint32_t);
+  const size_t dsm = (size_t)dwpc * dense_words(k3all) * sizeof(uint32_t);
   const unsigned gd = (unsigned)std::max<int64_t>(
       1, std::min<int64_t>((nd_cap + dwpc - 1) / dwpc, (int64_t)kSMs * 64 / dwpc));
   auto befriend = [&](auto fp32_tag, auto vl_tag) {
@@ -1557,7 +1591,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         run_g, b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(), sc, (uint32_t)nd_cap,
         b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c,
-        (uint32_t)k3all);
+        (uint32_t)dense_words(k3all));
     CMH_LAUNCHED();
     k_befriend_simple<PT, FP, VL><<<rg(k_befriend_simple<PT, FP, VL>, npc), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), run_g,
@@ -1780,7 +1814,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   // shared memory of the dense-top kernel: one parent per fine cell of a top
   // cell (set here, outside any graph capture)
   {
-    const int dsm = (int)(dense_warps_per_cta(k3all) * k3all * sizeof(uint32_t));
+    const int dsm = (int)(dense_warps_per_cta(k3all) * dense_words(k3all) * sizeof(uint32_t));
     const void *dense[] = {
         (const void *)k_befriend_dense<float, true, false>,
         (const void *)k_befriend_dense<float, false, false>,

@@ -148,6 +148,18 @@ using cmh::Plan;
   }
 
 namespace {
+// The caller's current device; CMH_ERR_NO_DEVICE when there is none (or no
+// usable driver), rather than the runtime's error text.
+int current_device() {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    (void)cudaGetLastError();
+    cmh::fail(CMH_ERR_NO_DEVICE, "no usable CUDA device");
+  }
+  int dev = 0;
+  CMH_CUDA(cudaGetDevice(&dev));
+  return dev;
+}
 
 void check_parts(const cmh_particles *parts) {
   if (!parts) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "particles is NULL");
@@ -324,8 +336,7 @@ cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
   if (!params || !cat) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "params and catalog are required");
   check_parts(parts);
   memset(cat, 0, sizeof *cat);
-  int dev = 0;
-  CMH_CUDA(cudaGetDevice(&dev));
+  const int dev = current_device();
   std::unique_ptr<Plan> pl(new Plan(*params, parts->pos_dtype, dev));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cmh_particles dp = *parts;
@@ -421,8 +432,7 @@ cmh_status cmh_fof_run_batch(const cmh_fof_params *params, const cmh_particles *
     cmh::fail(CMH_ERR_INVALID_ARGUMENT, "params, particles and catalogs are required");
   for (int b = 0; b < nbox; b++) memset(&cats[b], 0, sizeof cats[b]);
   if (nbox == 0) return CMH_OK;
-  int dev = 0;
-  CMH_CUDA(cudaGetDevice(&dev));
+  const int dev = current_device();
   std::unique_ptr<Plan> pl(new Plan(params[0], parts[0].pos_dtype, dev));
   pl->use_graph = false;
   run_batch_on(*pl, params, parts, nbox, cats, static_cast<cudaStream_t>(stream));

@@ -73,15 +73,22 @@ void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n,
 // ---- radix_sort.cu -----------------------------------------------------------
 // Stable LSD radix sort of (key u64, value u32) pairs on the low `bits` key
 // bits.  Result lands in keys/vals (the alt buffers are scratch); `tmp`
-// holds the digit count tables and `scan_tmp` the scratch of their scan.
+// holds the digit counts and the tiles' look-back states.
 // `n` sizes the launches; with `n_dev` set, the element count is read from
 // device memory (at most n), so the sort needs no host synchronisation.
+// `tmp` must already hold radix_sort_scratch(n) bytes when the sort is
+// captured in a graph; `giveups` (device) counts capped look-back waits.
+// With copy_back false and an odd number of 8-bit passes the result stays in
+// keys_alt/vals_alt (no copy).
 void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s);
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s,
+                        bool copy_back = true);
 // Same for 32-bit keys.
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s);
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s);
+// Scratch bytes of a sort of up to n keys.
+size_t radix_sort_scratch(int64_t n);
 
 }  // namespace cmh

@@ -1506,6 +1506,11 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaMemsetAsync(b_boxd.p, 0, 7 * sizeof(uint32_t) * nbox, s));
 
   // ---- ingest ----
+  // keys and indices are emitted where an odd number of sort passes starts,
+  // so that the last pass lands in b_keys / b_vals
+  const bool odd = ((key_bits + 7) / 8) % 2 == 1;
+  uint64_t *emit_k = odd ? b_keys_alt.as<uint64_t>() : b_keys.as<uint64_t>();
+  uint32_t *emit_v = odd ? b_vals_alt.as<uint32_t>() : b_vals.as<uint32_t>();
   if (n > 0) {
     k_ingest_count<PT><<<rg(k_ingest_count<PT>, n), kT, 0, s>>>(boxes, nbox, n, keep,
                                                       nimg);
@@ -1522,13 +1527,15 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     k_ingest_emit<PT><<<rg(k_ingest_emit<PT>, n), kT, 0, s>>>(
         boxes, nbox, n, k3all, keep, keep_scan,
         img_scan, nimg, boxd, (uint32_t)npc,
-        b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>());
+        emit_k, emit_v, b_ppos.as<SPos<PT>>());
     CMH_LAUNCHED();
   }
   mark(0);
   // ---- sort ----
-  radix_sort_u64_u32(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(), b_keys_alt.as<uint64_t>(),
-                     b_vals_alt.as<uint32_t>(), npc, &sc->np, key_bits, sort_tmp, scan_tmp, s);
+  // the sort ends in b_keys / b_vals without a copy
+  radix_sort_u64_u32(emit_k, emit_v, odd ? b_keys.as<uint64_t>() : b_keys_alt.as<uint64_t>(),
+                     odd ? b_vals.as<uint32_t>() : b_vals_alt.as<uint32_t>(), npc, &sc->np,
+                     key_bits, sort_tmp, &c->sort_giveups, s, false);
   mark(1);
   // ---- runs, top-cell ranges, dense maps ----
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
@@ -1671,7 +1678,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_LAUNCHED();
   radix_sort_u32_u32(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), b_okeys_alt.as<uint32_t>(),
                      b_ovals_alt.as<uint32_t>(), ncc, &sc->nh, bits_for((uint64_t)npc),
-                     sort_tmp, scan_tmp, s);
+                     sort_tmp, &c->sort_giveups, s);
   CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, (size_t)ncc * 4, s));
 #define CMH_CATALOG(NSV)                                                                        \
   k_catalog<NSV><<<rg(k_catalog<NSV>, ncc), kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc,          \
@@ -1835,14 +1842,8 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
       m = (m + 4095) / 4096;
       need += 2 * m;
     }
-    const int64_t ntiles = (npc + 4095) / 4096;
-    int64_t need_h = 0;
-    for (int64_t m = ntiles * 256; m > 4096;) {
-      m = (m + 4095) / 4096;
-      need_h += 2 * m;
-    }
-    scan_tmp.ensure((size_t)(std::max(need, need_h) + 16) * sizeof(uint32_t));
-    sort_tmp.ensure((size_t)(2 * ntiles * 256 + 64) * sizeof(uint32_t));
+    scan_tmp.ensure((size_t)(need + 16) * sizeof(uint32_t));
+    sort_tmp.ensure(radix_sort_scratch(std::max(npc, ncc)));
   }
 }
 
@@ -1862,6 +1863,8 @@ void Plan::read_back(cudaStream_t s, bool timed) {
   last = hs_;
   if (hc.c.uf_giveups)
     fail(CMH_ERR_DEVICE_TIMEOUT, "union-find retry loop reached its iteration cap");
+  if (hc.c.sort_giveups)
+    fail(CMH_ERR_DEVICE_TIMEOUT, "radix sort look-back wait reached its cap");
   stats = cmh_stats{};
   stats.n_in = n_total;
   stats.n_out = n_total - hs_.kept_total;

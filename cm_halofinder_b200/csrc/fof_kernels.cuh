@@ -89,6 +89,7 @@ struct Counters {
   unsigned long long find_steps;   // parent loads in the befriending finds
   unsigned long long scan_iters;   // fine cells scanned in sparse top cells
   unsigned long long window_iters; // map slots visited in dense top cells
+  unsigned int sort_giveups;       // radix-sort look-back waits that hit their cap
 };
 
 // FP32 band around l^2: returns the thresholds t_lo < fl32(l2) < t_hi such

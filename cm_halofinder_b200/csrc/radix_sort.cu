@@ -1,10 +1,12 @@
 // Stable LSD radix sort of (key, value) pairs, 8-bit digits.
 //
-// Per digit pass: (1) each 4096-key tile counts its digits in shared memory;
-// (2) the digit-major count table (256 x tiles) is prefix-summed, giving each
-// (digit, tile) its output offset; (3) each tile ranks its keys stably with
-// warp match/ballot counters, stages them in shared memory in digit order and
-// writes each digit's run contiguously (coalesced) to its offset.
+// One read of the keys counts the digits of every pass (k_rs_upfront), which
+// gives each digit's start in the output.  Each pass is then a single
+// kernel: each 4096-key tile ranks its keys stably with warp match/ballot
+// counters, learns how many keys of each digit the lower tiles hold by
+// decoupled look-back over published tile states, stages its keys in shared
+// memory in digit order and writes each digit's run contiguously
+// (coalesced).
 #include <algorithm>
 
 #include "cmh_internal.cuh"
@@ -17,6 +19,12 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kIPT = 16;
 constexpr int kTile = kThreads * kIPT;  // 4096
 constexpr int kBins = 256;
+constexpr int kMaxPasses = 8;
+// Tile states of the look-back, one 64-bit word per (tile, digit): the flag
+// in the high half, the count in the low half, written in one store.
+constexpr uint64_t kAggregate = 1ull << 32;  // count = the tile's own keys of the digit
+constexpr uint64_t kInclusive = 2ull << 32;  // count = keys of the digit up to this tile
+constexpr int kSpinCap = 1 << 22;            // polls of one state before giving up
 
 template <class K>
 __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
@@ -48,28 +56,45 @@ __device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t *warp_s
   return inc - v + warp_sums[warp];
 }
 
+// All digit histograms of the sort in one read of the keys: pass p's 256
+// counters at ghist[256 p].
 template <class K>
-__global__ void __launch_bounds__(kThreads) k_rs_hist(const K *__restrict__ keys, int64_t n_cap,
-                                                      const uint32_t *__restrict__ n_dev,
-                                                      int shift, uint32_t *__restrict__ hist,
-                                                      int64_t ntiles) {
-  __shared__ uint32_t h[kBins];
+__global__ void __launch_bounds__(kThreads) k_rs_upfront(const K *__restrict__ keys,
+                                                         int64_t n_cap,
+                                                         const uint32_t *__restrict__ n_dev,
+                                                         int passes,
+                                                         uint32_t *__restrict__ ghist) {
+  __shared__ uint32_t h[kMaxPasses * kBins];
   const int64_t n = n_dev ? (int64_t)*n_dev : n_cap;
-  h[threadIdx.x] = 0;
+  for (int i = threadIdx.x; i < passes * kBins; i += kThreads) h[i] = 0;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kTile;
-#pragma unroll 4
-  for (int j = 0; j < kIPT; j++) {
-    int64_t i = base + (int64_t)j * kThreads + threadIdx.x;
-    if (i < n) atomicAdd(&h[digit_of(keys[i], shift)], 1u);
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * kThreads) {
+    const K k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&h[p * kBins + digit_of(k, 8 * p)], 1u);
   }
   __syncthreads();
-  hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+  for (int i = threadIdx.x; i < passes * kBins; i += kThreads)
+    if (h[i]) atomicAdd(&ghist[i], h[i]);
 }
 
-// The scatter pass ranks a 4096-key tile with 512 threads x 8 keys: fewer
-// registers per thread than the counting pass's layout, so more warps hide
-// the memory latency.
+// Exclusive prefix over the digits of each pass (one CTA per pass).
+__global__ void __launch_bounds__(kThreads) k_rs_offsets(const uint32_t *__restrict__ ghist,
+                                                         uint32_t *__restrict__ goff) {
+  __shared__ uint32_t warp_sums[kWarps];
+  const uint32_t v = ghist[blockIdx.x * kBins + threadIdx.x];
+  goff[blockIdx.x * kBins + threadIdx.x] = block_exclusive(v, warp_sums);
+}
+
+// One digit pass, single sweep: a CTA takes the next tile from a counter
+// (so every lower tile is already being worked on), ranks its 4096 keys
+// stably in shared memory (512 threads x 8 keys; warp match/ballot counters),
+// publishes its per-digit counts, then finds the counts of all lower tiles
+// by looking back through their published states (decoupled look-back:
+// inclusive states end the walk) and writes each digit's run contiguously to
+// goff[digit] + (keys of the digit in lower tiles).  A tile publishes its own
+// counts before it waits on anything, so every wait ends; a wait is still
+// capped, and a capped one sets *giveups.
 constexpr int kSThreads = 512;
 constexpr int kSWarps = kSThreads / 32;
 constexpr int kSIPT = kTile / kSThreads;  // 8
@@ -81,25 +106,45 @@ struct ScatterSmem {
   uint32_t wcnt[kSWarps][kBins];
   uint32_t dstart[kBins];
   uint32_t gofs[kBins];
+  uint32_t thist[kBins];
   uint32_t warp_sums[kSWarps];
+  uint32_t tile;
 };
+
+// Lanes of the warp with the same 9-bit value d (a digit, or kBins for an
+// empty slot): one ballot per bit.
+__device__ __forceinline__ uint32_t peers_of(uint32_t d) {
+  uint32_t peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 9; b++) {
+    const uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+    peers &= ((d >> b) & 1u) ? m : ~m;
+  }
+  return peers;
+}
+
+__device__ __forceinline__ uint64_t load_state(const uint64_t *p) {
+  return *reinterpret_cast<const volatile uint64_t *>(p);
+}
 
 template <class K>
 __global__ void __launch_bounds__(kSThreads) k_rs_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
     K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n_cap,
-    const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ hist_scan,
-    int64_t ntiles) {
+    const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ goff,
+    uint64_t *__restrict__ state, uint32_t *__restrict__ tile_ctr,
+    unsigned int *__restrict__ giveups) {
   const int64_t n = n_dev ? (int64_t)*n_dev : n_cap;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem<K> &sm = *reinterpret_cast<ScatterSmem<K> *>(smem_raw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t base = (int64_t)blockIdx.x * kTile;
-
+  if (threadIdx.x == 0) sm.tile = atomicAdd(tile_ctr, 1u);
   for (int i = threadIdx.x; i < kSWarps * kBins; i += kSThreads) (&sm.wcnt[0][0])[i] = 0;
-  if (threadIdx.x < kBins) sm.gofs[threadIdx.x] = hist_scan[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+  if (threadIdx.x < kBins) sm.thist[threadIdx.x] = 0;
   __syncthreads();
-
+  const uint32_t tile = sm.tile;
+  const int64_t base = (int64_t)tile * kTile;
+  if (base >= n) return;  // the whole CTA leaves together
   const uint32_t lt_mask = (1u << lane) - 1u;
   K k[kSIPT];
   uint32_t v[kSIPT], rank[kSIPT];
@@ -109,8 +154,23 @@ __global__ void __launch_bounds__(kSThreads) k_rs_scatter(
     const bool valid = i < n;
     k[j] = valid ? keys_in[i] : K(0);
     v[j] = valid ? vals_in[i] : 0u;
+  }
+  // the tile's digit counts first, published before the ranking so that
+  // the higher tiles' look-back finds them early
+#pragma unroll
+  for (int j = 0; j < kSIPT; j++)
+    if (base + (int64_t)warp * 32 * kSIPT + j * 32 + lane < n)
+      atomicAdd(&sm.thist[digit_of(k[j], shift)], 1u);
+  __syncthreads();
+  if (threadIdx.x < kBins)
+    atomicExch(reinterpret_cast<unsigned long long *>(state + (uint64_t)tile * kBins + threadIdx.x),
+               (unsigned long long)((tile == 0 ? kInclusive : kAggregate) | sm.thist[threadIdx.x]));
+#pragma unroll
+  for (int j = 0; j < kSIPT; j++) {
+    const int64_t i = base + (int64_t)warp * 32 * kSIPT + j * 32 + lane;
+    const bool valid = i < n;
     const uint32_t d = valid ? digit_of(k[j], shift) : (uint32_t)kBins;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = peers_of(d);
     const uint32_t lt = peers & lt_mask;
     uint32_t c = 0;
     if (valid) c = sm.wcnt[warp][d];
@@ -141,7 +201,28 @@ __global__ void __launch_bounds__(kSThreads) k_rs_scatter(
       if (lane < kSWarps) sm.warp_sums[lane] = wi - w;
     }
     __syncthreads();
-    if (d < kBins) sm.dstart[d] = inc - acc + sm.warp_sums[warp];
+    if (d < kBins) {
+      sm.dstart[d] = inc - acc + sm.warp_sums[warp];
+      // add up the lower tiles' counts, then publish the running total
+      uint64_t *mine = state + (uint64_t)tile * kBins + d;
+      uint32_t excl = 0;
+      if (tile != 0) {
+        for (int64_t j = (int64_t)tile - 1; j >= 0; j--) {
+          const uint64_t *p = state + (uint64_t)j * kBins + d;
+          uint64_t w = load_state(p);
+          for (int spin = 0; (w >> 32) == 0 && spin < kSpinCap; spin++) w = load_state(p);
+          if ((w >> 32) == 0) {
+            atomicAdd(giveups, 1u);
+            break;
+          }
+          excl += (uint32_t)w;
+          if ((w >> 32) == 2) break;
+        }
+        atomicExch(reinterpret_cast<unsigned long long *>(mine),
+                   (unsigned long long)(kInclusive | (uint64_t)(excl + acc)));
+      }
+      sm.gofs[d] = goff[d] + excl;
+    }
   }
   __syncthreads();
   const int64_t rem = n - base;
@@ -168,17 +249,30 @@ __global__ void __launch_bounds__(kSThreads) k_rs_scatter(
 
 template <class K>
 void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, int64_t n,
-                     const uint32_t *n_dev, int bits, DevBuf &tmp, DevBuf &scan_tmp,
-                     cudaStream_t s) {
-  if (n <= 1 || bits <= 0) return;
+                     const uint32_t *n_dev, int bits, DevBuf &tmp, unsigned int *giveups,
+                     cudaStream_t s, bool copy_back) {
+  if (bits <= 0) return;
   const int passes = (bits + 7) / 8;
+  if (n <= 1) {
+    // nothing to order; still leave the data where the caller expects it
+    if (!copy_back && passes % 2 == 1 && n == 1) {
+      CMH_CUDA(cudaMemcpyAsync(keys_alt, keys, sizeof(K), cudaMemcpyDeviceToDevice, s));
+      CMH_CUDA(cudaMemcpyAsync(vals_alt, vals, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    }
+    return;
+  }
+  if (passes > kMaxPasses || bits > (int)(8 * sizeof(K)))
+    fail(CMH_ERR_INVALID_ARGUMENT, "radix sort: key bits out of range");
   const int64_t ntiles = (n + kTile - 1) / kTile;
-  const int64_t hn = ntiles * kBins;
-  if (hn > 0xffffffffll) fail(CMH_ERR_CAPACITY, "radix sort: too many tiles");
-  // layout of tmp: hist | hist_scan | scan scratch (own buffer)
-  tmp.ensure((size_t)(2 * hn + 64) * sizeof(uint32_t));
-  uint32_t *hist = tmp.as<uint32_t>();
-  uint32_t *hist_scan = hist + hn;
+  if (ntiles >= 0xffffffffll) fail(CMH_ERR_CAPACITY, "radix sort: too many tiles");
+  // tmp: tile states (ntiles x 256 u64) | digit counts | digit offsets | tile counters
+  const size_t state_bytes = (size_t)ntiles * kBins * sizeof(uint64_t);
+  const size_t small = (size_t)(2 * kMaxPasses * kBins + kMaxPasses) * sizeof(uint32_t);
+  tmp.ensure(radix_sort_scratch(n));
+  uint64_t *state = tmp.as<uint64_t>();
+  uint32_t *ghist = reinterpret_cast<uint32_t *>(tmp.as<unsigned char>() + state_bytes);
+  uint32_t *goff = ghist + kMaxPasses * kBins;
+  uint32_t *tile_ctr = goff + kMaxPasses * kBins;
   const size_t smem = sizeof(ScatterSmem<K>);
   {
     // once per device, never inside a graph capture
@@ -193,20 +287,25 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
       done[dev] = true;
     }
   }
+  CMH_CUDA(cudaMemsetAsync(ghist, 0, small, s));
+  k_rs_upfront<K><<<grid_resident(reinterpret_cast<const void *>(k_rs_upfront<K>), kThreads, 0,
+                                  n),
+                    kThreads, 0, s>>>(keys, n, n_dev, passes, ghist);
+  CMH_LAUNCHED();
+  k_rs_offsets<<<passes, kThreads, 0, s>>>(ghist, goff);
+  CMH_LAUNCHED();
   K *src_k = keys, *dst_k = keys_alt;
   uint32_t *src_v = vals, *dst_v = vals_alt;
   for (int p = 0; p < passes; p++) {
-    const int shift = 8 * p;
-    k_rs_hist<K><<<(unsigned)ntiles, kThreads, 0, s>>>(src_k, n, n_dev, shift, hist, ntiles);
-    CMH_LAUNCHED();
-    exclusive_scan_u32(hist, hist_scan, hn, nullptr, scan_tmp, s);
-    k_rs_scatter<K><<<(unsigned)ntiles, kSThreads, smem, s>>>(src_k, src_v, dst_k, dst_v, n,
-                                                              n_dev, shift, hist_scan, ntiles);
+    CMH_CUDA(cudaMemsetAsync(state, 0, state_bytes, s));
+    k_rs_scatter<K><<<(unsigned)ntiles, kSThreads, smem, s>>>(
+        src_k, src_v, dst_k, dst_v, n, n_dev, 8 * p, goff + p * kBins, state, tile_ctr + p,
+        giveups);
     CMH_LAUNCHED();
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);
   }
-  if (src_k != keys) {
+  if (src_k != keys && copy_back) {
     CMH_CUDA(cudaMemcpyAsync(keys, src_k, (size_t)n * sizeof(K), cudaMemcpyDeviceToDevice, s));
     CMH_CUDA(cudaMemcpyAsync(vals, src_v, (size_t)n * sizeof(uint32_t),
                              cudaMemcpyDeviceToDevice, s));
@@ -215,16 +314,24 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
 
 }  // namespace
 
+size_t radix_sort_scratch(int64_t n) {
+  const int64_t ntiles = (std::max<int64_t>(n, 1) + kTile - 1) / kTile;
+  return (size_t)ntiles * kBins * sizeof(uint64_t) +
+         (size_t)(2 * kMaxPasses * kBins + kMaxPasses) * sizeof(uint32_t);
+}
+
 void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s) {
-  radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, scan_tmp, s);
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s, bool copy_back) {
+  radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
+                            copy_back);
 }
 
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, DevBuf &scan_tmp, cudaStream_t s) {
-  radix_sort_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, scan_tmp, s);
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s) {
+  radix_sort_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
+                            true);
 }
 
 }  // namespace cmh

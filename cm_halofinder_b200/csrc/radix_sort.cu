@@ -128,7 +128,7 @@ __device__ __forceinline__ uint64_t load_state(const uint64_t *p) {
 }
 
 template <class K>
-__global__ void __launch_bounds__(kSThreads) k_rs_scatter(
+__global__ void __launch_bounds__(kSThreads, 3) k_rs_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
     K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n_cap,
     const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ goff,

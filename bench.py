@@ -127,6 +127,19 @@ def describe(args, w, dtype, n):
             f"{w.meta['n_clumps']} clumps, l={w.linklength:.6f}, Boundarysize={w.boundary}")
 
 
+# DRAM bytes per processed particle of the befriending launches (ncu, 256^3
+# box at scale 1/2: 479.3 MB for 8,971,801 processed particles)
+BEFRIEND_DRAM_PER_PROC = 479.27e6 / 8971801
+
+# the launches behind each stage's CUDA-event interval
+KERNELS = {
+    "befriend": "befriending stage: k_befriend_dense + k_befriend_simple + 2 x k_befriend "
+                "(near, far) + 2 x k_compress",
+    "sort": "radix sort: k_rs_upfront + 5 x k_rs_scatter",
+    "ingest": "k_ingest_count + 2 scans + k_ingest_emit",
+}
+
+
 def stage_bytes(st, pos_bytes):
     """Algorithmic bytes per stage (the minimum data each stage must move in
     this design): see the measurement section of the design notes."""
@@ -289,10 +302,21 @@ def run_ours(args):
     sb = stage_bytes(st, pos_bytes)
     dominant = max(sb, key=lambda k: stages.get(k, 0.0))
     ach = sb[dominant] / (stages[dominant] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1),
+    traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
+    if traffic is None and dominant == "befriend" and args.config in ("c2", "c5"):
+        # DRAM bytes of the befriending launches per processed particle, from
+        # the ncu capture summarised in profiles/befriend_c2_half.md
+        traffic = int(BEFRIEND_DRAM_PER_PROC * st["n_proc"])
+        traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the stage's six "
+                       "launches on the box at scale 1/2 (profiles/befriend_c2_half.md), "
+                       "scaled by processed particles")
+    roofline = {"bound": "hbm", "kernel": KERNELS.get(dominant, dominant),
+                "achieved": round(ach, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": round(ach / peak, 4), "traffic": args.traffic,
+                "frac": round(ach / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": int(sb[dominant]),
+                "timing": "CUDA events around the stage's launches on the caller's stream, "
+                          "eager step after the timed region",
                 "stage_gbs": {k: round(sb[k] / (stages[k] * 1e-3) / 1e9, 1)
                               for k in sb if stages.get(k, 0) > 0}}
 

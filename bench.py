@@ -141,8 +141,8 @@ KERNELS = {
 
 
 def stage_bytes(st, pos_bytes):
-    """Algorithmic bytes per stage (the minimum data each stage must move in
-    this design): see the measurement section of the design notes."""
+    """Algorithmic bytes per stage: the data each stage must move in this
+    design (processed particles npr, fine cells R, position record rec)."""
     n, npr, R = st["n_in"], st["n_proc"], st["n_cells"]
     passes = (st["key_bits"] + 7) // 8
     rec = 16 if pos_bytes == 4 else 32
@@ -305,11 +305,10 @@ def run_ours(args):
     traffic, traffic_src = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and dominant == "befriend" and args.config in ("c2", "c5"):
         # DRAM bytes of the befriending launches per processed particle, from
-        # the ncu capture summarised in profiles/befriend_c2_half.md
+        # an ncu capture of the 256^3 box at scale 1/2
         traffic = int(BEFRIEND_DRAM_PER_PROC * st["n_proc"])
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the stage's six "
-                       "launches on the box at scale 1/2 (profiles/befriend_c2_half.md), "
-                       "scaled by processed particles")
+                       "launches on the 256^3 box at scale 1/2, scaled by processed particles")
     roofline = {"bound": "hbm", "kernel": KERNELS.get(dominant, dominant),
                 "achieved": round(ach, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",

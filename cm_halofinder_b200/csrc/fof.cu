@@ -642,9 +642,10 @@ __device__ __forceinline__ uint32_t bit_span(int lo, int hi) {
 // cell's faces are left to the global passes.  The occupied fine cells of
 // the top cell are first marked in bit rows (bit x of rows[z k + y]), so a
 // cell visits only the occupied cells of its forward window, a row at a
-// time, and reads the fine-cell map only for those.  `tid`/`nt` number the
+// time, and finds their local indices from the rows' prefix counts (no map
+// read).  `tid`/`nt` number the
 // threads that share the top cell and `sync` is their barrier; `lpar` holds
-// k3all parents followed by the k^2 rows.
+// k3all parents followed by the k^2 rows and their k^2 prefix counts.
 template <class PT, bool FP32, bool VL, class Sync>
 __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_t tid,
                                           uint32_t nt, Sync sync, const BoxDev *boxes,
@@ -657,9 +658,11 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
   const uint32_t f = fr.x, n = fr.y - fr.x;
   const Geom &g = boxes[run_box[f]].g;
   const int k = g.k, W = g.W;
-  uint32_t *rows = lpar + k3all;
+  const uint32_t nrow = (uint32_t)(k * k);
+  uint32_t *rows = lpar + k3all;   // occupancy bits of each (z, y) row
+  uint32_t *pref = rows + nrow;    // occupied fine cells before each row
   for (uint32_t i = tid; i < n; i += nt) lpar[i] = i;
-  for (uint32_t j = tid; j < (uint32_t)(k * k); j += nt) rows[j] = 0u;
+  for (uint32_t j = tid; j < nrow; j += nt) rows[j] = 0u;
   sync();
   for (uint32_t i = tid; i < n; i += nt) {
     const uint64_t pg = run_g[f + i];
@@ -668,7 +671,26 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
              1u << (gx - div_k(gx, g) * k));
   }
   sync();
-  const int32_t *map = maps + (uint64_t)slot * k3all;
+  if (tid < 32) {
+    // the top cell's fine cells are in sub-cell order, so a cell's local
+    // index is the number of occupied cells in the rows before it plus those
+    // before it in its row: prefix of the row populations, one warp
+    const uint32_t per = (nrow + 31) / 32, j0 = tid * per, j1 = min(j0 + per, nrow);
+    uint32_t sum = 0;
+    for (uint32_t j = j0; j < j1; j++) sum += __popc(rows[j]);
+    uint32_t inc = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, d);
+      if (tid >= (uint32_t)d) inc += t;
+    }
+    uint32_t acc = inc - sum;
+    for (uint32_t j = j0; j < j1; j++) {
+      pref[j] = acc;
+      acc += __popc(rows[j]);
+    }
+  }
+  sync();
   for (int pass = 0; pass < 2; pass++) {
     for (uint32_t i = tid; i < n; i += nt) {
       const uint32_t a = f + i;
@@ -680,6 +702,7 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
       const uint32_t reach = bit_span(max(sx - W, 0), min(sx + W, k - 1));
       const uint32_t near = bit_span(max(sx - 1, 0), min(sx + 1, k - 1));
       const uint32_t after = sx == 31 ? 0u : (0xffffffffu << (sx + 1));
+      uint32_t ri = lfind(lpar, i);  // may go stale: re-found before a pair test
       for (int dz = 0; dz <= W && sz + dz < k; dz++)
         for (int dy = (dz == 0 ? 0 : -W); dy <= W; dy++) {
           const int ty = sy + dy;
@@ -690,22 +713,22 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
           else m = rc <= 1 ? (reach & ~near) : reach;   // Chebyshev distance >= 2
           if (dz == 0 && dy == 0) m &= after;           // forward only in a's own row
           const int tz = sz + dz;
-          uint32_t bits = rows[tz * k + ty] & m;
+          const uint32_t row = (uint32_t)(tz * k + ty);
+          const uint32_t occ = rows[row];
+          uint32_t bits = occ & m;
           while (bits) {
             const int tx = __ffs(bits) - 1;
             bits &= bits - 1u;
-            const int32_t r = map[(tz * k + ty) * k + tx];
-            if (r < 0) continue;
+            const uint32_t lj = pref[row] + __popc(occ & ((1u << tx) - 1u));
             st.cand++;
-            const uint32_t lj = (uint32_t)r - f;
-            const uint32_t ri = lfind(lpar, i), rj = lfind(lpar, lj);
-            if (ri == rj) {
+            const uint32_t rj = lfind(lpar, lj);
+            if (rj == ri || rj == (ri = lfind(lpar, i))) {
               st.skips++;
               continue;
             }
             auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
-            if (cells_linked<PT, FP32, VL>(g, (uint32_t)r, gx + (tx - sx), gy + dy, gz + dz, sa,
-                                           ea, run_start, spos, svl, st, apart)) {
+            if (cells_linked<PT, FP32, VL>(g, f + lj, gx + (tx - sx), gy + dy, gz + dz, sa, ea,
+                                           run_start, spos, svl, st, apart)) {
               lunion(lpar, ri, rj, ctr);
               st.unions++;
             }
@@ -1452,10 +1475,11 @@ template <class K> unsigned rg(K *kernel, int64_t n) {
   return grid_resident(reinterpret_cast<const void *>(kernel), kT, 0, n);
 }
 
-// Shared-memory words of one dense top cell: k^3 parents and k^2 bit rows.
+// Shared-memory words of one dense top cell: k^3 parents, k^2 bit rows and
+// k^2 row prefixes.
 uint64_t dense_words(uint64_t k3all) {
   const uint64_t k = (uint64_t)std::llround(std::cbrt((double)k3all));
-  return k3all + k * k;
+  return k3all + 2 * k * k;
 }
 
 // Warps per CTA of the dense-top kernel: up to 4, each with the words of one

@@ -12,7 +12,7 @@ the band; the plain FP64 form is measured on the same box and reported
 beside it.  With N GPUs (torchrun) every rank runs its own box (weak
 scaling; the boxes are independent domains, there is no exchange).
 Before timing, the plan's autotuner picks the cell-size scale and the
-dense-map threshold on the same box (--no-autotune keeps the defaults).
+dense-top threshold on the same box (--no-autotune keeps the defaults).
 
 Other workloads: --config c1 (64^3, FP64 positions), c3 (50M-particle
 lightcone with a variable linking length), c4 (64 batched boxes, 61M
@@ -365,7 +365,7 @@ def run_batched(args):
     """64 independent periodic boxes of uneven size in one batched run per
     step (one sort, one befriending pass, one reduction over all boxes),
     replayed from a captured CUDA graph, after the autotuner has picked the
-    cell-size scale and the dense-map threshold."""
+    cell-size scale and the dense-top threshold."""
     import torch
     from cm_halofinder_b200 import FofConfig, Plan, synth
 
@@ -596,7 +596,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="issue every step eagerly")
     ap.add_argument("--no-autotune", action="store_true",
-                    help="skip the autotuner (default cell-size factor and dense-map threshold)")
+                    help="skip the autotuner (default cell-size factor and dense-top threshold)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-timeout", type=float, default=20.0)
     ap.add_argument("--traffic", type=float, default=None,

@@ -241,7 +241,7 @@ class Plan:
         return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
 
     def autotune(self, configs, positions, velocities, repeats=2, stream=None):
-        """Time the boxes over a grid of cell-size scales and dense-map
+        """Time the boxes over a grid of cell-size scales and dense-top
         thresholds; the plan keeps the fastest.  Returns the choice."""
         nb, P, parts, _keep = self._batch_args(configs, positions, velocities)
         t = _abi.Tuning()

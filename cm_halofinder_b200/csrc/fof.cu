@@ -395,41 +395,31 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
 // the others by one warp each.
 constexpr uint32_t kBigTop = 128;
 
-// Fine-cell maps of the dense top cells (the first nd_cap of them; a dense
-// top cell without a map is scanned instead, which is slower but exact).
-// The slots of the big ones are listed in `big`.
-__global__ void __launch_bounds__(kT) k_dense_maps(const uint64_t *__restrict__ run_g,
-                                                   const uint16_t *__restrict__ run_box,
-                                                   const BoxDev *__restrict__ boxes,
-                                                   DevScal *sc, uint64_t k3all,
-                                                   const uint2 *__restrict__ top_range,
-                                                   const uint32_t *__restrict__ dflag,
-                                                   const uint32_t *__restrict__ dscan,
-                                                   uint32_t dense_min, uint32_t nd_cap,
-                                                   uint32_t *__restrict__ top_slot,
-                                                   uint2 *__restrict__ dense_range,
-                                                   uint32_t *__restrict__ big,
-                                                   int32_t *__restrict__ maps) {
+// Slots of the dense top cells (the first nd_cap of them; a dense top cell
+// without a slot is scanned instead, which is slower but exact): the top
+// cell's slot and fine-cell range; the slots of the big ones are listed in
+// `big`.  One thread per top cell's first fine cell.
+__global__ void __launch_bounds__(kT) k_dense_slots(const uint64_t *__restrict__ run_g,
+                                                    const uint16_t *__restrict__ run_box,
+                                                    const BoxDev *__restrict__ boxes,
+                                                    DevScal *sc,
+                                                    const uint2 *__restrict__ top_range,
+                                                    const uint32_t *__restrict__ dflag,
+                                                    const uint32_t *__restrict__ dscan,
+                                                    uint32_t nd_cap,
+                                                    uint32_t *__restrict__ top_slot,
+                                                    uint2 *__restrict__ dense_range,
+                                                    uint32_t *__restrict__ big) {
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
-    const BoxDev &bx = boxes[run_box[r]];
-    const uint64_t pg = run_g[r];
-    const uint64_t t = top_of_run(bx, pg);
-    const uint2 tr = top_range[t];
-    const uint32_t f = tr.x;
-    if (tr.y - f <= dense_min) continue;
-    const uint32_t slot = dscan[f];  // the first fine cell of the top cell carries the slot
+    if (!dflag[r]) continue;
+    const uint32_t slot = dscan[r];
     if (slot >= nd_cap) continue;
-    if (dflag[r]) {
-      top_slot[t] = slot;
-      dense_range[slot] = tr;
-      if (tr.y - f > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
-    }
-    const int k = bx.g.k;
-    const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-    const uint64_t sub = ((uint64_t)(gz - div_k(gz, bx.g) * k) * k + (gy - div_k(gy, bx.g) * k)) * k +
-                         (gx - div_k(gx, bx.g) * k);
-    maps[(uint64_t)slot * k3all + sub] = (int32_t)r;
+    const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
+    const uint2 tr = top_range[t];
+    top_slot[t] = slot;
+    dense_range[slot] = tr;
+    if (tr.y - tr.x > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
   }
 }
 
@@ -642,8 +632,7 @@ __device__ __forceinline__ uint32_t bit_span(int lo, int hi) {
 // cell's faces are left to the global passes.  The occupied fine cells of
 // the top cell are first marked in bit rows (bit x of rows[z k + y]), so a
 // cell visits only the occupied cells of its forward window, a row at a
-// time, and finds their local indices from the rows' prefix counts (no map
-// read).  `tid`/`nt` number the
+// time, and finds their local indices from the rows' prefix counts.  `tid`/`nt` number the
 // threads that share the top cell and `sync` is their barrier; `lpar` holds
 // k3all parents followed by the k^2 rows and their k^2 prefix counts.
 template <class PT, bool FP32, bool VL, class Sync>
@@ -651,9 +640,10 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
                                           uint32_t nt, Sync sync, const BoxDev *boxes,
                                           const uint16_t *run_box, uint64_t k3all,
                                           const uint32_t *run_start, const uint64_t *run_g,
-                                          const uint2 *dense_range, const int32_t *maps,
-                                          const SPos<PT> *spos, const VLRec<FP32> *svl,
-                                          uint32_t *parent, Counters *ctr, BfStats &st) {
+                                          const uint2 *dense_range, uint32_t *grows,
+                                          uint32_t kk, const SPos<PT> *spos,
+                                          const VLRec<FP32> *svl, uint32_t *parent,
+                                          Counters *ctr, BfStats &st) {
   const uint2 fr = dense_range[slot];
   const uint32_t f = fr.x, n = fr.y - fr.x;
   const Geom &g = boxes[run_box[f]].g;
@@ -738,6 +728,13 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
     sync();
   }
   for (uint32_t i = tid; i < n; i += nt) parent[f + i] = f + lfind(lpar, i);
+  // rows and prefixes stay for the warp path, which looks up this top
+  // cell's fine cells from its neighbours
+  uint32_t *gr = grows + (uint64_t)slot * 2 * kk;
+  for (uint32_t j = tid; j < nrow; j += nt) {
+    gr[j] = rows[j];
+    gr[kk + j] = pref[j];
+  }
   sync();
 }
 
@@ -752,8 +749,9 @@ __global__ void __launch_bounds__(128) k_befriend_dense(
     const BoxDev *__restrict__ boxes, const uint16_t *__restrict__ run_box, uint64_t k3all,
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint2 *__restrict__ dense_range, const uint32_t *__restrict__ big, DevScal *sc,
-    uint32_t nd_cap, const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
-    const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr, uint32_t lstride) {
+    uint32_t nd_cap, uint32_t *__restrict__ grows, uint32_t kk,
+    const SPos<PT> *__restrict__ spos, const VLRec<FP32> *__restrict__ svl, uint32_t *parent,
+    Counters *ctr, uint32_t lstride) {
   extern __shared__ uint32_t smem[];
   __shared__ uint32_t s_slot;
   const uint32_t nd = min(sc->nd, nd_cap), nbig = sc->nbig;
@@ -769,7 +767,7 @@ __global__ void __launch_bounds__(128) k_befriend_dense(
     __syncthreads();
     if (slot == kNone) break;
     dense_top<PT, FP32, VL>(slot, smem, threadIdx.x, blockDim.x, cta_sync, boxes, run_box,
-                            k3all, run_start, run_g, dense_range, maps, spos, svl, parent,
+                            k3all, run_start, run_g, dense_range, grows, kk, spos, svl, parent,
                             ctr, st);
   }
   const uint32_t lane = threadIdx.x & 31;
@@ -783,7 +781,7 @@ __global__ void __launch_bounds__(128) k_befriend_dense(
     const uint2 fr = dense_range[slot];
     if (fr.y - fr.x > kBigTop) continue;
     dense_top<PT, FP32, VL>(slot, lpar, lane, 32, warp_sync, boxes, run_box, k3all, run_start,
-                            run_g, dense_range, maps, spos, svl, parent, ctr, st);
+                            run_g, dense_range, grows, kk, spos, svl, parent, ctr, st);
   }
   st.flush(ctr);
 }
@@ -906,9 +904,9 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
 
 // Warp path, one warp per queued fine cell a.  Lanes 0..13 fetch the 14
 // top-cell ranges at once; the candidate slots of all 14 (fine cells of small
-// top cells, map slots of the window in mapped ones) are then flattened and
-// taken 32 at a time, so a cell costs a few L2 round trips instead of one per
-// slot.  Warps take cells from an atomic counter as they finish, so a few
+// top cells, window slots of dense ones, found through their occupancy rows)
+// are then flattened and taken 32 at a time, so a cell costs a few L2 round
+// trips instead of one per slot.  Warps take cells from an atomic counter as they finish, so a few
 // expensive cells do not hold back a whole static share.  PHASE 0 visits the
 // candidates within one fine cell, PHASE 1 the farther ones, so that a dense
 // neighbourhood is joined (and compressed) before its far pairs are tried and
@@ -919,7 +917,7 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
     const uint32_t *__restrict__ run_start, const uint64_t *__restrict__ run_g,
     const uint32_t *__restrict__ queue, DevScal *sc, const uint2 *__restrict__ top_range,
     const uint32_t *__restrict__ top_slot,
-    const int32_t *__restrict__ maps, const SPos<PT> *__restrict__ spos,
+    const uint32_t *__restrict__ grows, uint32_t kk, const SPos<PT> *__restrict__ spos,
     const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr) {
   const uint32_t NQ = sc->qcount;
   uint32_t *next = PHASE == 0 ? &sc->next0 : &sc->next1;
@@ -953,7 +951,7 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
         const uint32_t f = tr.x, e = tr.y;
         const uint32_t slot = top_slot[tb];
         r0 = lane == 0 ? a + 1 : f;
-        // pairs inside a mapped top cell are joined by k_befriend_dense
+        // pairs inside a dense top cell are joined by k_befriend_dense
         if (lane == 0 && slot != kNone) r0 = e;
         if (r0 < e) {
           if (slot == kNone) {
@@ -1020,10 +1018,14 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
         bx2 = l_x0 + (int)(sl % (uint32_t)l_nx);
         by2 = l_y0 + (int)((sl / (uint32_t)l_nx) % (uint32_t)l_ny);
         bz2 = l_z0 + (int)(sl / (uint32_t)(l_nx * l_ny));
-        const int32_t rr = maps[(uint64_t)l_map * k3all +
-                                (uint64_t)(((bz2 - l_oz) * k + (by2 - l_oy)) * k + (bx2 - l_ox))];
-        if (rr < 0 || (uint32_t)rr < l_r0) continue;
-        r = (uint32_t)rr;
+        // occupancy bit of the slot's fine cell, then its index from the
+        // top cell's row prefix (fine cells are in sub-cell order)
+        const uint32_t *gr = grows + (uint64_t)l_map * 2 * kk;
+        const uint32_t row = (uint32_t)((bz2 - l_oz) * k + (by2 - l_oy));
+        const uint32_t occ = gr[row];
+        const int cx = bx2 - l_ox;
+        if (!((occ >> cx) & 1u)) continue;
+        r = l_r0 + gr[kk + row] + __popc(occ & ((1u << cx) - 1u));
       }
       const int cheb = max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz)));
       if ((PHASE == 0 && cheb > 1) || (PHASE == 1 && cheb <= 1)) continue;
@@ -1489,10 +1491,16 @@ int dense_warps_per_cta(uint64_t k3all) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(4, (200u << 10) / per));
 }
 
-// Dense top cells whose fine-cell maps fit in 8 bytes per processed particle
-// plus 1 GiB.
-int64_t maps_cap_for(int64_t np_cap, uint64_t k3all) {
-  return (int64_t)(((uint64_t)np_cap * 8 + (1ull << 30)) / (k3all * 4));
+// Occupancy rows of a top cell (k^2).
+uint64_t rows_per_top(uint64_t k3all) {
+  const uint64_t k = (uint64_t)std::llround(std::cbrt((double)k3all));
+  return k * k;
+}
+
+// Dense top cells whose rows and row prefixes fit in 4 bytes per processed
+// particle plus 1 GiB.
+int64_t rows_cap_for(int64_t np_cap, uint64_t k3all) {
+  return (int64_t)(((uint64_t)np_cap * 4 + (1ull << 30)) / (rows_per_top(k3all) * 8));
 }
 
 // Images per input particle expected for a periodic box (the shell's share
@@ -1561,7 +1569,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                      odd ? b_vals.as<uint32_t>() : b_vals_alt.as<uint32_t>(), npc, &sc->np,
                      key_bits, sort_tmp, &c->sort_giveups, s, false);
   mark(1);
-  // ---- runs, top-cell ranges, dense maps ----
+  // ---- runs, top-cell ranges, dense top cells ----
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
   uint32_t *run_scan = flag + npc;
   k_gather_flags<PT><<<rg(k_gather_flags<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(),
@@ -1596,21 +1604,19 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s);
   k_clamp_dense<<<1, 32, 0, s>>>(sc, (uint32_t)nd_cap);
   CMH_LAUNCHED();
-  CMH_CUDA(cudaMemsetAsync(b_maps.p, 0xff, (size_t)nd_cap * k3all * 4, s));
-  k_dense_maps<<<rg(k_dense_maps, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                 k3all, b_top_range.as<uint2>(),
-                                 b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), dense_min,
-                                 (uint32_t)nd_cap, b_top_slot.as<uint32_t>(),
-                                 b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(),
-                                 b_maps.as<int32_t>());
+  k_dense_slots<<<rg(k_dense_slots, npc), kT, 0, s>>>(
+      run_g, b_run_box.as<uint16_t>(), boxes, sc, b_top_range.as<uint2>(),
+      b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), (uint32_t)nd_cap,
+      b_top_slot.as<uint32_t>(), b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>());
   CMH_LAUNCHED();
   k_iota<<<rg(k_iota, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
   mark(2);
   // ---- befriending: dense top cells inside (CTA each), fast path, queue,
   // warp path near then far ----
-  uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense maps
+  uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense slots
   const int dwpc = dense_warps_per_cta(k3all);
+  const uint32_t kk = (uint32_t)rows_per_top(k3all);
   const size_t dsm = (size_t)dwpc * dense_words(k3all) * sizeof(uint32_t);
   const unsigned gd = (unsigned)std::max<int64_t>(
       1, std::min<int64_t>((nd_cap + dwpc - 1) / dwpc, (int64_t)kSMs * 64 / dwpc));
@@ -1621,7 +1627,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     k_befriend_dense<PT, FP, VL><<<gd, 32 * dwpc, dsm, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         run_g, b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(), sc, (uint32_t)nd_cap,
-        b_maps.as<int32_t>(), b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c,
+        b_rows.as<uint32_t>(), kk, b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c,
         (uint32_t)dense_words(k3all));
     CMH_LAUNCHED();
     k_befriend_simple<PT, FP, VL><<<rg(k_befriend_simple<PT, FP, VL>, npc), kT, 0, s>>>(
@@ -1632,16 +1638,14 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     k_befriend<PT, FP, VL, 0><<<rg(k_befriend<PT, FP, VL, 0>, npc * 32), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         run_g, queue, sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
-        b_maps.as<int32_t>(),
-        b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
+        b_rows.as<uint32_t>(), kk, b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
     k_compress<<<rg(k_compress, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
     CMH_LAUNCHED();
     k_befriend<PT, FP, VL, 1><<<rg(k_befriend<PT, FP, VL, 1>, npc * 32), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         run_g, queue, sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
-        b_maps.as<int32_t>(),
-        b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
+        b_rows.as<uint32_t>(), kk, b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c);
     CMH_LAUNCHED();
   };
   if (fp32 && varlink) befriend(std::true_type{}, std::true_type{});
@@ -1790,10 +1794,10 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   // capacities: grown after a run that overflowed them, never shrunk
   const int64_t want_np = std::min<int64_t>(n_total + (int64_t)img, (int64_t)0xfffffff0ll);
   np_cap = std::max<int64_t>(np_cap, std::max<int64_t>(want_np, 1));
-  // fine-cell maps of dense top cells: at most 8 bytes per processed
-  // particle plus 1 GiB (dense top cells past the cap are scanned instead)
+  // dense top cells: their rows take at most 4 bytes per processed particle
+  // plus 1 GiB (dense top cells past the cap are scanned instead)
   nd_cap = std::max<int64_t>(nd_cap, np_cap / 1024 + 1024);
-  nd_cap = std::min<int64_t>(nd_cap, std::max<int64_t>(1024, maps_cap_for(np_cap, k3all)));
+  nd_cap = std::min<int64_t>(nd_cap, std::max<int64_t>(1024, rows_cap_for(np_cap, k3all)));
   double mincut = 1e300;
   for (const BoxDev &bd : boxes_host) mincut = std::min(mincut, bd.g.nphalomin);
   const int64_t div = (int64_t)std::max(1.0, std::floor(mincut));
@@ -1818,7 +1822,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   b_top_slot.ensure(n_top * 4);
   b_rtmp1.ensure(npc * 4);
   b_rtmp2.ensure(npc * 4);
-  b_maps.ensure((size_t)nd_cap * k3all * 4);
+  b_rows.ensure((size_t)nd_cap * rows_per_top(k3all) * 2 * sizeof(uint32_t));
   b_dense_range.ensure((size_t)nd_cap * sizeof(uint2));
   b_dense_big.ensure((size_t)nd_cap * sizeof(uint32_t));
   b_parent.ensure(npc * 4);
@@ -1964,9 +1968,9 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
       if (!(last.overflow & 1u) && use_graph) capture(want_member, s, sig);
     }
     stats.n_launches = launches_per_run;
-    if (last.overflow & 2u)  // faster next time, within the map budget
+    if (last.overflow & 2u)  // faster next time, within the rows budget
       nd_cap = std::min<int64_t>((int64_t)last.nd + last.nd / 4 + 256,
-                                 std::max<int64_t>(nd_cap, maps_cap_for(np_cap, k3all)));
+                                 std::max<int64_t>(nd_cap, rows_cap_for(np_cap, k3all)));
     if (!(last.overflow & 1u)) return;
     np_cap = (int64_t)last.np_raw + last.np_raw / 8 + 4096;  // repeat with room
   }
@@ -1999,7 +2003,7 @@ void Plan::capture(bool want_member, cudaStream_t s, const std::vector<unsigned 
   (void)s;
 }
 
-// Grid search over the cell-size scale and the dense-map threshold, timing
+// Grid search over the cell-size scale and the dense-top threshold, timing
 // eager runs of the real boxes (after one untimed run per setting, which
 // also grows the buffers).  The fastest setting stays in the plan.
 cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaStream_t s) {
@@ -2013,7 +2017,7 @@ cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaSt
       cell_scale = sc;
       dense_min = dm;
       // each setting starts from an empty workspace, so that one setting's
-      // large buffers (many top cells, or large maps) do not stay allocated
+      // large buffers (many top cells, or many dense ones) do not stay allocated
       // under the next; a setting that does not fit in memory is skipped
       release_workspace();
       float t = 0;

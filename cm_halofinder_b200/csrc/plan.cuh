@@ -61,7 +61,7 @@ struct Plan : public cmh_plan {
   DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
   DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_svl;
   DevBuf b_run_start, b_run_box, b_top_range, b_top_slot, b_rtmp1, b_rtmp2;
-  DevBuf b_maps, b_dense_range, b_dense_big;
+  DevBuf b_rows, b_dense_range, b_dense_big;
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
@@ -72,7 +72,7 @@ struct Plan : public cmh_plan {
     DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd,
                      &b_keys, &b_keys_alt, &b_vals, &b_vals_alt, &b_ppos, &b_spos, &b_svl,
                      &b_run_start, &b_run_box, &b_top_range, &b_top_slot,
-                     &b_rtmp1, &b_rtmp2, &b_maps, &b_dense_range, &b_dense_big, &b_parent, &b_count,
+                     &b_rtmp1, &b_rtmp2, &b_rows, &b_dense_range, &b_dense_big, &b_parent, &b_count,
                      &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
                      &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
                      &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,

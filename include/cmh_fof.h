@@ -111,8 +111,8 @@ typedef struct cmh_stats {
   int64_t n_unions;        /* ... joined by a linked particle pair            */
   int64_t n_find_steps;    /* union-find parent loads while befriending       */
   int64_t n_scan_iters;    /* fine cells scanned in sparse top cells          */
-  int64_t n_window_iters;  /* map slots visited in dense top cells            */
-  int64_t n_dense_tops;    /* top cells with a fine-cell map                  */
+  int64_t n_window_iters;  /* window slots visited in dense top cells         */
+  int64_t n_dense_tops;    /* top cells joined in shared memory (dense)       */
 } cmh_stats;
 
 /* Halo catalog in the layout of the reference's unformatted records
@@ -186,12 +186,12 @@ cmh_status cmh_plan_set_graph(cmh_plan *plan, int32_t enable);
 
 /* Autotuner: times runs of these boxes (device-resident, as for
  * cmh_plan_run_batch) over a grid of cell-size scales (fine cells per
- * top-cell edge relative to one particle per top cell) and dense-map
+ * top-cell edge relative to one particle per top cell) and dense-top
  * thresholds, `repeats` timed runs each, and keeps the fastest setting in
  * the plan for its later runs.  Boxes whose params set cell_factor keep it. */
 typedef struct cmh_tuning {
   double cell_scale;   /* chosen scale of the cell-size factor            */
-  int32_t dense_min;   /* chosen occupied-fine-cell threshold for a map   */
+  int32_t dense_min;   /* occupied fine cells above which a top cell is dense */
   float ms;            /* best run time (CUDA events)                     */
   int32_t tried;       /* settings timed                                  */
 } cmh_tuning;

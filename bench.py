@@ -160,16 +160,9 @@ def run_ours(args):
     import torch
     from cm_halofinder_b200 import FofConfig, Plan, synth
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from cm_halofinder_b200.replicas import Replicas
+    rep = Replicas("nccl")
+    rank, world, local = rep.rank, rep.world, rep.local
     dev = torch.device("cuda", local)
     if args.config == "c5":
         # 1024^3: drawn on the device (host generation would take minutes)
@@ -181,21 +174,12 @@ def run_ours(args):
         pos = torch.from_numpy(w.pos).to(dev)
         vel = torch.from_numpy(w.vel).to(dev)
     n = int(pos.shape[0])
+    n_all = rep.sum(n)  # particles of all ranks' boxes
     np_dtype = np.float32 if pos.dtype == torch.float32 else np.float64
     in_bytes = pos.numel() * pos.element_size() + vel.numel() * vel.element_size()
     stream = torch.cuda.current_stream(dev)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    def max_ranks(ms):
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+    barrier, max_ranks = rep.barrier, rep.max
 
     def timed(plan, steps, warmup):
         for _ in range(warmup):
@@ -236,7 +220,7 @@ def run_ours(args):
     ms, st, launches = timed(plan, args.steps, 0)
     clk = clocks.stop()
     stages = stage_breakdown(plan)
-    value = n * world / (ms * 1e-3) / 1e6
+    value = n_all / (ms * 1e-3) / 1e6
     cat_fast = plan.run(pos, vel, out="host", stream=stream)
     plan.close()
 
@@ -261,7 +245,7 @@ def run_ours(args):
             a = cat_p.props[:, 1:4].astype(np.float64)
             b = cat_fast.props[:, 1:4].astype(np.float64)
             rel = float(np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-30)))
-        plain = {"value": n * world / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
+        plain = {"value": n_all / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
                  "n_pair_tests": st_p["n_pair_tests"],
                  "stage_ms": {k: round(v, 4) for k, v in stages_p.items()},
                  "speedup_of_chosen_form": ms_p / ms,
@@ -294,7 +278,7 @@ def run_ours(args):
     barrier()
     plan.close()
     ms_e2e = max_ranks(e0.elapsed_time(e1) / args.steps)
-    e2e = {"value": n * world / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+    e2e = {"value": n_all / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": int(in_bytes), "d2h_bytes_per_step": int(d2h)}
 
     peak, peak_kind = peaks()
@@ -327,9 +311,7 @@ def run_ours(args):
                              "256^3 box give the reference's rate)"}
         else:
             cpu = cpu_baseline(w, args.cpu_seconds)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     if rank != 0:
         return
     line = {
@@ -369,16 +351,9 @@ def run_batched(args):
     import torch
     from cm_halofinder_b200 import FofConfig, Plan, synth
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from cm_halofinder_b200.replicas import Replicas
+    rep = Replicas("nccl")
+    rank, world, local = rep.rank, rep.world, rep.local
     boxes = synth.config4(seed=4 + 1000 * rank, scale=args.scale)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
@@ -386,18 +361,9 @@ def run_batched(args):
     pos = [torch.from_numpy(w.pos).to(dev) for w in boxes]
     vel = [torch.from_numpy(w.vel).to(dev) for w in boxes]
     n = sum(w.n for w in boxes)
+    n_all = rep.sum(n)  # particles of all ranks' boxes
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    def max_ranks(ms):
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+    barrier, max_ranks = rep.barrier, rep.max
 
     def timed(plan, steps, warmup, inputs):
         for _ in range(warmup):
@@ -425,7 +391,7 @@ def run_batched(args):
     ms, cats, nh = timed(plan, args.steps, 0, resident)
     clk = clocks.stop()
     st = cats[0].stats
-    value = n * world / (ms * 1e-3) / 1e6
+    value = n_all / (ms * 1e-3) / 1e6
 
     plain = None
     if not args.no_plain and args.precision != "fp64":
@@ -445,7 +411,7 @@ def run_batched(args):
         e1.record(stream)
         barrier()
         ms_p = max_ranks(e0.elapsed_time(e1) / max(1, args.steps))
-        plain = {"value": n * world / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
+        plain = {"value": n_all / (ms_p * 1e-3) / 1e6, "ms_per_step": ms_p,
                  "speedup_of_chosen_form": ms_p / ms}
         plan_p.close()
 
@@ -462,12 +428,10 @@ def run_batched(args):
 
     ms_e2e, _, _ = timed(plan, args.steps, max(1, args.warmup), copied)
     d2h = sum(c.props.nbytes + c.head.nbytes for c in cats)
-    e2e = {"value": n * world / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+    e2e = {"value": n_all / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": int(sum(w.pos.nbytes + w.vel.nbytes for w in boxes)),
            "d2h_bytes_per_step": int(d2h)}
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     if rank != 0:
         return
     ns = [w.n for w in boxes]

@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
 
 // Dense top cells with more fine cells than this are joined by a whole CTA,
 // the others by one warp each.
-constexpr uint32_t kBigTop = 128;
+constexpr uint32_t kBigTop = 64;
 
 // Slots of the dense top cells (the first nd_cap of them; a dense top cell
 // without a slot is scanned instead, which is slower but exact): the top

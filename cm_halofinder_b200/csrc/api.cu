@@ -93,6 +93,9 @@ Plan::~Plan() {
   cudaSetDevice(device);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (cap_stream) cudaStreamDestroy(cap_stream);
+  if (side_stream) cudaStreamDestroy(side_stream);
+  if (ev_side_start) cudaEventDestroy(ev_side_start);
+  if (ev_vel_ready) cudaEventDestroy(ev_vel_ready);
   each_buf([](DevBuf &b) { b.release(); });
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -296,12 +299,28 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog 
     const size_t vb = (size_t)parts->n * 3 * (parts->vel_dtype == CMH_FLOAT64 ? 8 : 4);
     pl.in_pos.ensure(pb);
     pl.in_vel.ensure(vb);
+    if (!pl.side_stream) {
+      CMH_CUDA(cudaStreamCreateWithFlags(&pl.side_stream, cudaStreamNonBlocking));
+      CMH_CUDA(cudaEventCreateWithFlags(&pl.ev_side_start, cudaEventDisableTiming));
+      CMH_CUDA(cudaEventCreateWithFlags(&pl.ev_vel_ready, cudaEventDisableTiming));
+    }
+    // positions on the caller's stream; velocities on the side stream once
+    // the caller's earlier work (the previous run's sums read in_vel) is done
+    CMH_CUDA(cudaEventRecord(pl.ev_side_start, s));
+    CMH_CUDA(cudaStreamWaitEvent(pl.side_stream, pl.ev_side_start, 0));
     CMH_CUDA(cudaMemcpyAsync(pl.in_pos.p, parts->pos, pb, cudaMemcpyHostToDevice, s));
-    CMH_CUDA(cudaMemcpyAsync(pl.in_vel.p, parts->vel, vb, cudaMemcpyHostToDevice, s));
+    CMH_CUDA(cudaMemcpyAsync(pl.in_vel.p, parts->vel, vb, cudaMemcpyHostToDevice,
+                             pl.side_stream));
+    CMH_CUDA(cudaEventRecord(pl.ev_vel_ready, pl.side_stream));
+    pl.vel_wait = true;
     dp.pos = pl.in_pos.p;
     dp.vel = pl.in_vel.p;
     dp.location = CMH_DEVICE;
   }
+  struct Reset {
+    Plan &p;
+    ~Reset() { p.vel_wait = false; }
+  } reset{pl};
   pl.run(dp, want_member != 0, s);
   if (out_location == CMH_DEVICE) catalog_on_device(pl, cat, want_member != 0);
   else catalog_to_host(pl, cat, want_member != 0, 0, s);

@@ -1675,6 +1675,15 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   mark(4);
 
   // ---- property sums, ownership, catalog ----
+  if (vel_wait) {
+    // host-resident velocities arrive on the side stream while the steps
+    // above run; the sums are their first reader
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CMH_CUDA(cudaStreamIsCapturing(s, &cs));
+    CMH_CUDA(cudaStreamWaitEvent(s, ev_vel_ready,
+                                 cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal
+                                                                     : cudaEventWaitDefault));
+  }
   const int NS = 6 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
   CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, s));
   CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, (size_t)ncc * 4, s));
@@ -1933,8 +1942,8 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     // the graph stays valid while the inputs, sizes and capacities do
     std::vector<unsigned char> sig(sizeof(BoxDev) * boxes_host.size());
     memcpy(sig.data(), boxes_host.data(), sig.size());
-    const int64_t caps[6] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
-                             (int64_t)dense_min};
+    const int64_t caps[7] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
+                             (int64_t)dense_min, (int64_t)vel_wait};
     sig.insert(sig.end(), (const unsigned char *)caps, (const unsigned char *)caps + sizeof caps);
     // and the workspace addresses the recorded launches use
     each_buf([&](DevBuf &b) {

@@ -56,6 +56,11 @@ struct Plan : public cmh_plan {
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<unsigned char> graph_sig;
   cudaStream_t cap_stream = nullptr;  // the stream runs are recorded on
+  // host-resident inputs: velocities are copied on a side stream while the
+  // run's first stages go on, and the property sums wait for them
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_side_start = nullptr, ev_vel_ready = nullptr;
+  bool vel_wait = false;
 
   // workspace
   DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;

@@ -73,7 +73,7 @@ def test_image_overflow_reruns_with_room():
 
 
 def test_autotune_keeps_results():
-    """The autotuner only changes cell sizes and the dense-map threshold; the
+    """The autotuner only changes cell sizes and the dense-top threshold; the
     catalogs after tuning match the oracle box by box."""
     import torch
     boxes = _boxes(5, 9)
@@ -101,3 +101,15 @@ def test_cell_scale_extremes(scale):
     cat = fof(w.pos, w.vel, FofConfig.from_workload(w, cell_factor=k), members=True)
     assert cat.stats["cell_factor"] == k
     assert_same_catalog(cat, ref)
+
+
+def test_host_inputs_repeated_runs_overlap_velocity_copy():
+    """Host-resident inputs: velocities are copied on a side stream while the
+    first stages run; eager, captured and replayed runs all match."""
+    w = synth.config2(seed=321, scale=40000 / 256 ** 3)
+    ref = cpu.run(w)
+    plan = Plan(FofConfig.from_workload(w))
+    for i in range(4):
+        vel = w.vel if i % 2 == 0 else w.vel.copy()  # a fresh host buffer every other run
+        cat = plan.run(w.pos, vel, members=True)
+        assert_same_catalog(cat, ref)

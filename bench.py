@@ -328,7 +328,8 @@ def run_ours(args):
                    "cell_pairs": st["n_cell_pairs"], "root_skips": st["n_root_skips"],
                    "unions": st["n_unions"], "find_steps": st["n_find_steps"],
                    "scan_iters": st["n_scan_iters"], "window_iters": st["n_window_iters"],
-                   "dense_tops": st["n_dense_tops"], "autotune": tune,
+                   "dense_tops": st["n_dense_tops"], "queued_cells": st["n_queued"],
+                   "big_tops": st["n_big_tops"], "autotune": tune,
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": f"inputs ({in_bytes / 1e6:.0f} MB) larger than L2; no flush"},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},

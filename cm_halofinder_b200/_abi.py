@@ -47,7 +47,8 @@ class Stats(C.Structure):
         ("cell_factor", C.c_int32), ("key_bits", C.c_int32), ("ms_total", C.c_float),
         ("stage_ms", C.c_float * 8), ("n_launches", C.c_int32)] + [
         (k, C.c_int64) for k in ("n_cell_pairs", "n_root_skips", "n_unions", "n_find_steps",
-                                 "n_scan_iters", "n_window_iters", "n_dense_tops")]
+                                 "n_scan_iters", "n_window_iters", "n_dense_tops",
+                                 "n_queued", "n_big_tops")]
 
     STAGES = ("ingest", "sort", "cells", "befriend", "groups", "sums", "catalog", "members")
 

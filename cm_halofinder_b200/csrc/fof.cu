@@ -1924,6 +1924,8 @@ void Plan::read_back(cudaStream_t s, bool timed) {
   stats.n_scan_iters = (int64_t)hc.c.scan_iters;
   stats.n_window_iters = (int64_t)hc.c.window_iters;
   stats.n_dense_tops = hs_.nd;
+  stats.n_queued = hs_.qcount;
+  stats.n_big_tops = hs_.nbig;
   if (timed) {
     float ms = 0;
     CMH_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));

@@ -113,6 +113,8 @@ typedef struct cmh_stats {
   int64_t n_scan_iters;    /* fine cells scanned in sparse top cells          */
   int64_t n_window_iters;  /* window slots visited in dense top cells         */
   int64_t n_dense_tops;    /* top cells joined in shared memory (dense)       */
+  int64_t n_queued;        /* fine cells sent to the warp-per-cell path       */
+  int64_t n_big_tops;      /* dense top cells joined by a whole CTA           */
 } cmh_stats;
 
 /* Halo catalog in the layout of the reference's unformatted records

@@ -27,7 +27,8 @@ from ._abi import (CMH_DEVICE, CMH_FLOAT32, CMH_FLOAT64, CMH_FP32_RECHECK, CMH_H
                    CMH_PLAIN_FP64, CMH_PROP_DISPERSION, CMH_PROP_INERTIA, CmhError)
 
 __all__ = [
-    "fof", "Plan", "Catalog", "FofConfig", "read_parameterfile", "write_halos", "write_info",
+    "fof", "Plan", "Catalog", "FofConfig", "read_parameterfile", "read_particles",
+    "config_from_run", "write_halos", "write_info",
     "CmhError", "CMH_FP32_RECHECK", "CMH_PLAIN_FP64", "CMH_PROP_INERTIA", "CMH_PROP_DISPERSION",
     "CMH_OUT_UNFORMATTED", "CMH_OUT_PARTICLES", "CMH_OUT_PARTICLE_ID", "halosize",
 ]
@@ -292,6 +293,37 @@ def read_parameterfile(fname, varlink=False):
     _abi.check(_abi.lib().cmh_read_parameterfile(str(fname).encode(), int(varlink),
                                                   C.byref(rp)))
     return rp
+
+
+_FORMATS = {"ascii": 0, "gadget1": 1, "picola_lightcone": 2}
+
+
+def read_particles(rp, fmt="ascii", with_id=False, fp64=False):
+    """Read every input file of a run (read_data.c:100-404) in the
+    reference's file order: returns (pos, vel, ids) host arrays, ids None
+    unless with_id.  fmt is "ascii", "gadget1" or "picola_lightcone"."""
+    L = _abi.lib()
+    parts = _abi.Particles()
+    store = C.c_void_p()
+    flags = (_abi.CMH_READ_PARTICLE_ID if with_id else 0) | (_abi.CMH_READ_FP64 if fp64 else 0)
+    _abi.check(L.cmh_read_particles(C.byref(rp), _FORMATS[fmt], flags, C.byref(parts),
+                                    C.byref(store)))
+    try:
+        n = int(parts.n)
+        dt = np.float64 if fp64 else np.float32
+        ct = C.c_double if fp64 else C.c_float
+
+        def arr(ptr, shape, ctype, dtype):
+            if n == 0:
+                return np.zeros(shape, dtype)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=shape).copy()
+
+        pos = arr(parts.pos, (n, 3), ct, dt)
+        vel = arr(parts.vel, (n, 3), ct, dt)
+        ids = arr(parts.id, (n,), C.c_uint64, np.uint64) if with_id else None
+    finally:
+        L.cmh_particle_store_free(store)
+    return pos, vel, ids
 
 
 def config_from_run(rp, task=0, periodic=False, precision="fp32", properties=0):

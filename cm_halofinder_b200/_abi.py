@@ -20,6 +20,8 @@ CMH_HOST, CMH_DEVICE = 0, 1
 CMH_PROP_INERTIA, CMH_PROP_DISPERSION = 1, 2
 CMH_OUT_UNFORMATTED, CMH_OUT_PARTICLES, CMH_OUT_PARTICLE_ID = 1, 2, 4
 CMH_TAGS_VARLINK, CMH_TAGS_INFOFILE = 1, 2
+CMH_FMT_ASCII, CMH_FMT_GADGET1, CMH_FMT_PICOLA_LIGHTCONE = 0, 1, 2
+CMH_READ_PARTICLE_ID, CMH_READ_FP64 = 1, 2
 
 
 class FofParams(C.Structure):
@@ -122,6 +124,9 @@ SIGNATURES = {
                                   C.POINTER(Particles), C.c_uint32]),
     "cmh_write_info": (C.c_int, [C.c_char_p, C.POINTER(RunParameters), C.POINTER(C.c_int64),
                                  C.c_int32]),
+    "cmh_read_particles": (C.c_int, [C.POINTER(RunParameters), C.c_int32, C.c_uint32,
+                                     C.POINTER(Particles), C.POINTER(C.c_void_p)]),
+    "cmh_particle_store_free": (None, [C.c_void_p]),
 }
 
 _lib = None

@@ -48,6 +48,12 @@ typedef double shim_real;
 #endif
 
 void FOF(void) {
+  if (cmh_abi_version() != CMH_ABI_VERSION) {
+    printf("\nERROR: libcmh_fof has ABI version %d, this program was built for %d; "
+           "rebuild it against the library's cmh_fof.h.\n\n",
+           cmh_abi_version(), CMH_ABI_VERSION);
+    FatalError((char *)"fof_shim.c", __LINE__);
+  }
 #ifdef VARLINK
   printf("\nERROR: the B200 FOF() does not support VARLINK builds.\n\n");
   FatalError((char *)"fof_shim.c", __LINE__);

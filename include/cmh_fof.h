@@ -18,7 +18,9 @@
 extern "C" {
 #endif
 
-#define CMH_ABI_VERSION 1
+/* Bumped whenever a structure's layout or an entry point's signature changes;
+ * a caller compares cmh_abi_version() with the value it was built against. */
+#define CMH_ABI_VERSION 2
 
 typedef enum cmh_status {
   CMH_OK = 0,
@@ -278,6 +280,27 @@ cmh_status cmh_read_parameterfile(const char *fname, int32_t build_flags,
  * Nx*Ny*Nz. */
 cmh_status cmh_params_from_run(const cmh_run_parameters *rp, int32_t task,
                                int32_t periodic, cmh_fof_params *out);
+
+/* ---- particle readers (read_data.c:100-404) ----------------------------- */
+
+#define CMH_FMT_ASCII 0             /* "[ID] x y z vx vy vz" lines (read_data.c:276-315, 368-404) */
+#define CMH_FMT_GADGET1 1           /* -DGADGET_STYLE snapshots (read_data.c:321-365)            */
+#define CMH_FMT_PICOLA_LIGHTCONE 2  /* -DLIGHTCONE -DUNFORMATTED files (read_data.c:212-273)     */
+#define CMH_READ_PARTICLE_ID 1u     /* -DPARTICLE_ID: the files carry IDs                        */
+#define CMH_READ_FP64 2u            /* no MEMORY_MODE: values kept (ASCII: read) as double       */
+
+typedef struct cmh_particle_store cmh_particle_store;
+
+/* Reads every input file of a run, in the reference's order: InputStyle 0
+ * reads "<InputFileBase>.<n>" for n = Starting_file .. Starting_file +
+ * Ninputfiles - 1, otherwise InputFileBase lists the files (read_data.c:
+ * 100-124, 178-198).  The particles of all files are appended in file order
+ * into host arrays that *store owns (free with cmh_particle_store_free); the
+ * domain filter and ghost images are left to the FoF run, which applies
+ * them as Read_Data does.  A missing or short file is CMH_ERR_IO. */
+cmh_status cmh_read_particles(const cmh_run_parameters *rp, int32_t format, uint32_t flags,
+                              cmh_particles *out, cmh_particle_store **store);
+void cmh_particle_store_free(cmh_particle_store *store);
 
 /* ---- catalog writers (FOF.c:546-957) ------------------------------------ */
 

@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol(native_lib):
     for name in declared_functions():
         assert hasattr(native_lib, name), name
     assert set(declared_functions()) == set(_abi.SIGNATURES)
-    assert native_lib.cmh_abi_version() == 1
+    assert native_lib.cmh_abi_version() == 2
 
 
 def test_structs_match_header_layout(tmp_path):

@@ -604,21 +604,23 @@ __device__ __forceinline__ uint32_t lfind(volatile uint32_t *lp, uint32_t x) {
   }
 }
 
-__device__ __forceinline__ void lunion(uint32_t *lp, uint32_t a, uint32_t b, Counters *ctr) {
+// Returns whether this call joined two components.
+__device__ __forceinline__ bool lunion(uint32_t *lp, uint32_t a, uint32_t b, Counters *ctr) {
   for (int it = 0; it < kUnionCap; it++) {
     a = lfind(lp, a);
     b = lfind(lp, b);
-    if (a == b) return;
+    if (a == b) return false;
     if (a < b) {
       const uint32_t t = a;
       a = b;
       b = t;
     }
     const uint32_t old = atomicCAS(lp + a, a, b);
-    if (old == a) return;
+    if (old == a) return true;
     a = old;
   }
   atomicAdd(&ctr->uf_giveups, 1u);
+  return false;
 }
 
 // Bits lo..hi (0 <= lo <= hi <= 31) set.
@@ -651,6 +653,9 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
   const uint32_t nrow = (uint32_t)(k * k);
   uint32_t *rows = lpar + k3all;   // occupancy bits of each (z, y) row
   uint32_t *pref = rows + nrow;    // occupied fine cells before each row
+  // components left: once one is left, every remaining candidate is joined
+  volatile uint32_t *ncomp = lpar + k3all + 2 * kk;
+  if (tid == 0) *ncomp = n;
   for (uint32_t i = tid; i < n; i += nt) lpar[i] = i;
   for (uint32_t j = tid; j < nrow; j += nt) rows[j] = 0u;
   sync();
@@ -683,6 +688,7 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
   sync();
   for (int pass = 0; pass < 2; pass++) {
     for (uint32_t i = tid; i < n; i += nt) {
+      if (*ncomp == 1) break;
       const uint32_t a = f + i;
       const uint64_t pg = run_g[a];
       const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
@@ -697,6 +703,7 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
         for (int dy = (dz == 0 ? 0 : -W); dy <= W; dy++) {
           const int ty = sy + dy;
           if (ty < 0 || ty >= k) continue;
+          if (*ncomp == 1) break;
           const int rc = max(abs(dy), dz);  // the row's distance in y and z
           uint32_t m;
           if (pass == 0) m = rc <= 1 ? near : 0u;       // Chebyshev distance <= 1
@@ -719,7 +726,7 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
             auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
             if (cells_linked<PT, FP32, VL>(g, f + lj, gx + (tx - sx), gy + dy, gz + dz, sa, ea,
                                            run_start, spos, svl, st, apart)) {
-              lunion(lpar, ri, rj, ctr);
+              if (lunion(lpar, ri, rj, ctr)) atomicSub(const_cast<uint32_t *>(ncomp), 1u);
               st.unions++;
             }
           }
@@ -1477,11 +1484,11 @@ template <class K> unsigned rg(K *kernel, int64_t n) {
   return grid_resident(reinterpret_cast<const void *>(kernel), kT, 0, n);
 }
 
-// Shared-memory words of one dense top cell: k^3 parents, k^2 bit rows and
-// k^2 row prefixes.
+// Shared-memory words of one dense top cell: k^3 parents, k^2 bit rows, k^2
+// row prefixes and the count of components.
 uint64_t dense_words(uint64_t k3all) {
   const uint64_t k = (uint64_t)std::llround(std::cbrt((double)k3all));
-  return k3all + 2 * k * k;
+  return k3all + 2 * k * k + 1;
 }
 
 // Warps per CTA of the dense-top kernel: up to 4, each with the words of one

@@ -144,11 +144,14 @@ def stage_bytes(st, pos_bytes):
     """Algorithmic bytes per stage: the data each stage must move in this
     design (processed particles npr, fine cells R, position record rec)."""
     n, npr, R = st["n_in"], st["n_proc"], st["n_cells"]
-    passes = (st["key_bits"] + 7) // 8
+    bits = st["key_bits"]
+    passes = (bits + 7) // 8
+    # passes reading 64-bit keys; the last of them writes 32-bit key words
+    wide = min(passes, max(1, -(-(bits - 32) // 8)))
     rec = 16 if pos_bytes == 4 else 32
     return {
         "ingest": 2 * 3 * pos_bytes * n + npr * (8 + 4 + rec),
-        "sort": passes * npr * 2 * (8 + 4),
+        "sort": npr * (8 + (wide - 1) * 24 + 20 + (passes - wide) * 16),
         "cells": npr * (4 + rec + rec + 8 + 4) + R * 12,
         "befriend": npr * rec + R * (8 + 4 + 4),
         "groups": npr * (4 + 4 + 4) + R * 12,

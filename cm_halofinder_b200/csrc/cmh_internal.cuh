@@ -84,6 +84,13 @@ void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s,
                         bool copy_back = true);
+// The values of the same sort, in key order, without the sorted keys: both
+// key buffers end as scratch (the later passes move 32-bit key words), and
+// the values end in vals_alt after an odd number of 8-bit passes, else in
+// vals.
+void radix_order_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
+                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
+                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s);
 // Same for 32-bit keys.
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,

@@ -173,10 +173,11 @@ __global__ void k_box_totals(const BoxDev *__restrict__ boxes, int nbox, int64_t
   if (np > np_cap) atomicOr(&sc->overflow, 1u);
 }
 
-template <class PT>
-__device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint64_t k3all,
-                                         uint32_t p, const double c[3], uint32_t src,
-                                         uint64_t *keys, uint32_t *vals, SPos<PT> *ppos) {
+// Fine-cell key of a processed particle at c: (top cell, counted over the
+// run's boxes) * k^3 + the fine cell within it.  c holds the stored (PT)
+// coordinates, so the key can be recomputed from the stored position.
+__device__ __forceinline__ uint64_t cell_key(const Geom &g, uint64_t top_base, uint64_t k3all,
+                                             const double c[3]) {
   int gi[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) gi[a] = fine_index(c[a], g.rmin[a], g.inv_h, g.G[a]);
@@ -184,7 +185,14 @@ __device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint6
   const int t[3] = {div_k(gi[0], g), div_k(gi[1], g), div_k(gi[2], g)};
   const uint64_t top = top_base + ((uint64_t)t[2] * g.T[1] + t[1]) * g.T[0] + t[0];
   const uint64_t sub = ((uint64_t)(gi[2] - t[2] * k) * k + (gi[1] - t[1] * k)) * k + (gi[0] - t[0] * k);
-  keys[p] = top * k3all + sub;
+  return top * k3all + sub;
+}
+
+template <class PT>
+__device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint64_t k3all,
+                                         uint32_t p, const double c[3], uint32_t src,
+                                         uint64_t *keys, uint32_t *vals, SPos<PT> *ppos) {
+  keys[p] = cell_key(g, top_base, k3all, c);
   vals[p] = p;
   SPos<PT> s;
   s.x = (PT)c[0];
@@ -259,24 +267,47 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
 // Runs of equal fine-cell keys.
 // ---------------------------------------------------------------------------
 
-// Cell-ordered positions and run-start flags; flags are 0 past the processed
-// count so that the scan over the capacity counts only real runs.
+// Fine-cell key of a stored processed particle: its stored coordinates are
+// those the key was emitted from, so the key is the emitted one exactly.
 template <class PT>
-__global__ void __launch_bounds__(kT) k_gather_flags(const uint64_t *__restrict__ keys,
-                                                     const uint32_t *__restrict__ perm,
+__device__ __forceinline__ uint64_t stored_key(const BoxDev *boxes, const uint64_t *s_base,
+                                               int nbox, uint64_t k3all, const SPos<PT> &sp) {
+  const BoxDev &bx = boxes[nbox > 1 ? box_search(s_base, nbox, (uint64_t)sp.src) : 0];
+  const double c[3] = {as_d(sp.x), as_d(sp.y), as_d(sp.z)};
+  return cell_key(bx.g, bx.top_base, k3all, c);
+}
+
+// Cell-ordered positions, their fine-cell keys (the sort leaves only the
+// order) and run-start flags; flags are 0 past the processed count so that
+// the scan over the capacity counts only real runs.  Lane l compares with
+// lane l-1's key; lane 0 recomputes its predecessor's.
+template <class PT>
+__global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict__ perm,
                                                      const SPos<PT> *__restrict__ ppos,
+                                                     const BoxDev *__restrict__ boxes, int nbox,
+                                                     uint64_t k3all,
                                                      SPos<PT> *__restrict__ spos,
+                                                     uint64_t *__restrict__ keys,
                                                      uint32_t *__restrict__ flag,
                                                      const DevScal *__restrict__ sc,
                                                      int64_t cap) {
+  __shared__ uint64_t s_base[kMaxBoxes];
+  load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
-  for (int64_t i = gtid(); i < cap; i += gstride()) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t w0 = gtid() - lane; w0 < cap; w0 += gstride()) {
+    const int64_t i = w0 + lane;
+    uint64_t key = 0;
     if (i < np) {
-      spos[i] = ppos[perm[i]];
-      flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
-    } else {
-      flag[i] = 0u;
+      const SPos<PT> sp = ppos[perm[i]];
+      spos[i] = sp;
+      key = stored_key<PT>(boxes, s_base, nbox, k3all, sp);
+      keys[i] = key;
     }
+    uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    if (lane == 0 && i > 0 && i < np)
+      prev = stored_key<PT>(boxes, s_base, nbox, k3all, ppos[perm[i - 1]]);
+    if (i < cap) flag[i] = (i < np && (i == 0 || key != prev)) ? 1u : 0u;
   }
 }
 
@@ -1546,7 +1577,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 
   // ---- ingest ----
   // keys and indices are emitted where an odd number of sort passes starts,
-  // so that the last pass lands in b_keys / b_vals
+  // so that the last pass leaves the indices in b_vals
   const bool odd = ((key_bits + 7) / 8) % 2 == 1;
   uint64_t *emit_k = odd ? b_keys_alt.as<uint64_t>() : b_keys.as<uint64_t>();
   uint32_t *emit_v = odd ? b_vals_alt.as<uint32_t>() : b_vals.as<uint32_t>();
@@ -1571,17 +1602,18 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   }
   mark(0);
   // ---- sort ----
-  // the sort ends in b_keys / b_vals without a copy
-  radix_sort_u64_u32(emit_k, emit_v, odd ? b_keys.as<uint64_t>() : b_keys_alt.as<uint64_t>(),
-                     odd ? b_vals.as<uint32_t>() : b_vals_alt.as<uint32_t>(), npc, &sc->np,
-                     key_bits, sort_tmp, &c->sort_giveups, s, false);
+  // the sort leaves the indices in cell order in b_vals and no sorted keys:
+  // k_gather_flags recomputes them into b_keys from the positions
+  radix_order_u64_u32(emit_k, emit_v, odd ? b_keys.as<uint64_t>() : b_keys_alt.as<uint64_t>(),
+                      odd ? b_vals.as<uint32_t>() : b_vals_alt.as<uint32_t>(), npc, &sc->np,
+                      key_bits, sort_tmp, &c->sort_giveups, s);
   mark(1);
   // ---- runs, top-cell ranges, dense top cells ----
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
   uint32_t *run_scan = flag + npc;
-  k_gather_flags<PT><<<rg(k_gather_flags<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), b_vals.as<uint32_t>(),
-                                       b_ppos.as<SPos<PT>>(), b_spos.as<SPos<PT>>(), flag, sc,
-                                       npc);
+  k_gather_flags<PT><<<rg(k_gather_flags<PT>, npc), kT, 0, s>>>(
+      b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>(), boxes, nbox, k3all, b_spos.as<SPos<PT>>(),
+      b_keys.as<uint64_t>(), flag, sc, npc);
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s);
   k_runs<<<rg(k_runs, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, boxes, nbox, k3all, sc,

@@ -6,7 +6,10 @@
 // counters, learns how many keys of each digit the lower tiles hold by
 // decoupled look-back over published tile states, stages its keys in shared
 // memory in digit order and writes each digit's run contiguously
-// (coalesced).
+// (coalesced).  A sort of 64-bit keys whose sorted keys are not wanted
+// narrows them to 32-bit words at the first pass after which at most 32 key
+// bits remain (the consumed low digits are dropped), so that the later
+// passes move 8 bytes per pair instead of 12.
 #include <algorithm>
 
 #include "cmh_internal.cuh"
@@ -127,11 +130,14 @@ __device__ __forceinline__ uint64_t load_state(const uint64_t *p) {
   return *reinterpret_cast<const volatile uint64_t *>(p);
 }
 
-template <class K>
+// Keys are read as K and written as KO = K >> out_shift (out_shift 0 unless
+// the pass narrows 64-bit keys to 32 bits).
+template <class K, class KO>
 __global__ void __launch_bounds__(kSThreads, 3) k_rs_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-    K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n_cap,
-    const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ goff,
+    KO *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n_cap,
+    const uint32_t *__restrict__ n_dev, int shift, int out_shift,
+    const uint32_t *__restrict__ goff,
     uint64_t *__restrict__ state, uint32_t *__restrict__ tile_ctr,
     unsigned int *__restrict__ giveups) {
   const int64_t n = n_dev ? (int64_t)*n_dev : n_cap;
@@ -242,15 +248,40 @@ __global__ void __launch_bounds__(kSThreads, 3) k_rs_scatter(
     const K key = sm.keys[q];
     const uint32_t d = digit_of(key, shift);
     const uint32_t g = sm.gofs[d] + (uint32_t)q - sm.dstart[d];
-    keys_out[g] = key;
+    keys_out[g] = (KO)(key >> out_shift);
     vals_out[g] = sm.vals[q];
   }
 }
 
+// Dynamic shared memory of every scatter instantiation, set once per device
+// (never inside a graph capture).
+void set_scatter_smem(cudaStream_t s) {
+  static bool done[64] = {};
+  int dev = 0;
+  CMH_CUDA(cudaGetDevice(&dev));
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CMH_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (dev >= 64 || done[dev] || cs != cudaStreamCaptureStatusNone) return;
+  CMH_CUDA(cudaFuncSetAttribute(k_rs_scatter<uint64_t, uint64_t>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem<uint64_t>)));
+  CMH_CUDA(cudaFuncSetAttribute(k_rs_scatter<uint64_t, uint32_t>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem<uint64_t>)));
+  CMH_CUDA(cudaFuncSetAttribute(k_rs_scatter<uint32_t, uint32_t>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScatterSmem<uint32_t>)));
+  done[dev] = true;
+}
+
+// With `narrow` (64-bit keys whose sorted order, not their sorted copy, is
+// wanted) the first m passes read 64-bit keys, m the fewest after which at
+// most 32 key bits remain; pass m-1 writes key >> 8m as 32-bit words and the
+// later passes sort those on the digits that are left.
 template <class K>
 void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, int64_t n,
                      const uint32_t *n_dev, int bits, DevBuf &tmp, unsigned int *giveups,
-                     cudaStream_t s, bool copy_back) {
+                     cudaStream_t s, bool copy_back, bool narrow) {
   if (bits <= 0) return;
   const int passes = (bits + 7) / 8;
   if (n <= 1) {
@@ -263,6 +294,8 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
   }
   if (passes > kMaxPasses || bits > (int)(8 * sizeof(K)))
     fail(CMH_ERR_INVALID_ARGUMENT, "radix sort: key bits out of range");
+  if (narrow && (copy_back || sizeof(K) != 8))
+    fail(CMH_ERR_INVALID_ARGUMENT, "radix sort: narrowing applies to 64-bit keys left unsorted");
   const int64_t ntiles = (n + kTile - 1) / kTile;
   if (ntiles >= 0xffffffffll) fail(CMH_ERR_CAPACITY, "radix sort: too many tiles");
   // tmp: tile states (ntiles x 256 u64) | digit counts | digit offsets | tile counters
@@ -273,20 +306,7 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
   uint32_t *ghist = reinterpret_cast<uint32_t *>(tmp.as<unsigned char>() + state_bytes);
   uint32_t *goff = ghist + kMaxPasses * kBins;
   uint32_t *tile_ctr = goff + kMaxPasses * kBins;
-  const size_t smem = sizeof(ScatterSmem<K>);
-  {
-    // once per device, never inside a graph capture
-    static bool done[64] = {};
-    int dev = 0;
-    CMH_CUDA(cudaGetDevice(&dev));
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    CMH_CUDA(cudaStreamIsCapturing(s, &cs));
-    if (dev < 64 && !done[dev] && cs == cudaStreamCaptureStatusNone) {
-      CMH_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-      done[dev] = true;
-    }
-  }
+  set_scatter_smem(s);
   CMH_CUDA(cudaMemsetAsync(ghist, 0, small, s));
   k_rs_upfront<K><<<grid_resident(reinterpret_cast<const void *>(k_rs_upfront<K>), kThreads, 0,
                                   n),
@@ -294,13 +314,27 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
   CMH_LAUNCHED();
   k_rs_offsets<<<passes, kThreads, 0, s>>>(ghist, goff);
   CMH_LAUNCHED();
-  K *src_k = keys, *dst_k = keys_alt;
+  // passes that read K keys; the rest read 32-bit keys
+  const int m = narrow ? std::min(passes, std::max(1, (bits - 32 + 7) / 8)) : passes;
+  void *src_k = keys, *dst_k = keys_alt;
   uint32_t *src_v = vals, *dst_v = vals_alt;
   for (int p = 0; p < passes; p++) {
     CMH_CUDA(cudaMemsetAsync(state, 0, state_bytes, s));
-    k_rs_scatter<K><<<(unsigned)ntiles, kSThreads, smem, s>>>(
-        src_k, src_v, dst_k, dst_v, n, n_dev, 8 * p, goff + p * kBins, state, tile_ctr + p,
-        giveups);
+    const uint32_t *go = goff + p * kBins;
+    if (p < m && !(narrow && p == m - 1)) {
+      k_rs_scatter<K, K><<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<K>), s>>>(
+          static_cast<const K *>(src_k), src_v, static_cast<K *>(dst_k), dst_v, n, n_dev, 8 * p,
+          0, go, state, tile_ctr + p, giveups);
+    } else if (p < m) {
+      k_rs_scatter<K, uint32_t><<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<K>), s>>>(
+          static_cast<const K *>(src_k), src_v, static_cast<uint32_t *>(dst_k), dst_v, n, n_dev,
+          8 * p, 8 * m, go, state, tile_ctr + p, giveups);
+    } else {
+      k_rs_scatter<uint32_t, uint32_t>
+          <<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<uint32_t>), s>>>(
+              static_cast<const uint32_t *>(src_k), src_v, static_cast<uint32_t *>(dst_k), dst_v,
+              n, n_dev, 8 * (p - m), 0, go, state, tile_ctr + p, giveups);
+    }
     CMH_LAUNCHED();
     std::swap(src_k, dst_k);
     std::swap(src_v, dst_v);
@@ -324,14 +358,21 @@ void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s, bool copy_back) {
   radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
-                            copy_back);
+                            copy_back, false);
+}
+
+void radix_order_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
+                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
+                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s) {
+  radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
+                            false, true);
 }
 
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s) {
   radix_sort_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
-                            true);
+                            true, false);
 }
 
 }  // namespace cmh

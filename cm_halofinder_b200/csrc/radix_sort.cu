@@ -131,9 +131,10 @@ __device__ __forceinline__ uint64_t load_state(const uint64_t *p) {
 }
 
 // Keys are read as K and written as KO = K >> out_shift (out_shift 0 unless
-// the pass narrows 64-bit keys to 32 bits).
+// the pass narrows 64-bit keys to 32 bits).  With 32-bit keys a CTA's shared
+// memory is small enough for 4 CTAs per SM.
 template <class K, class KO>
-__global__ void __launch_bounds__(kSThreads, 3) k_rs_scatter(
+__global__ void __launch_bounds__(kSThreads, sizeof(K) == 4 ? 4 : 3) k_rs_scatter(
     const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
     KO *__restrict__ keys_out, uint32_t *__restrict__ vals_out, int64_t n_cap,
     const uint32_t *__restrict__ n_dev, int shift, int out_shift,

@@ -117,30 +117,49 @@ __device__ __forceinline__ void load_pos(const BoxDev &bx, uint64_t li, double x
   x[2] = as_d(pos[3 * li + 2]);
 }
 
+// Keep flag (bit 0: inside the domain) and image count (bits 1..) of a
+// particle at x.
+template <class PT>
+__device__ __forceinline__ uint32_t ingest_flags(const Geom &g, const double x[3]) {
+  if (!in_domain(g, x)) return 0u;
+  uint32_t cnt = 0;
+  if (g.periodic) {
+    int opt[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      double c;
+      opt[a] = 1 + (int)image_coord<PT>(g, x[a], a, -1, &c) + (int)image_coord<PT>(g, x[a], a, 1, &c);
+    }
+    cnt = (uint32_t)(opt[0] * opt[1] * opt[2] - 1);
+  }
+  return 1u | (cnt << 1);
+}
+
+// Two particles per thread and step (i and i + stride), both positions
+// loaded before either is tested, so that each step waits on memory once.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_ingest_count(const BoxDev *__restrict__ boxes, int nbox,
                                                      int64_t n, uint32_t *__restrict__ keep,
                                                      uint32_t *__restrict__ nimg) {
   __shared__ uint64_t s_base[kMaxBoxes];
   load_bases(boxes, nbox, s_base, false);
-  for (int64_t i = gtid(); i < n; i += gstride()) {
-    const BoxDev &bx = boxes[box_search(s_base, nbox, (uint64_t)i)];
-    const Geom &g = bx.g;
-    double x[3];
-    load_pos<PT>(bx, (uint64_t)i - bx.in_base, x);
-    const bool ok = in_domain(g, x);
-    uint32_t cnt = 0;
-    if (ok && g.periodic) {
-      int opt[3];
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        double c;
-        opt[a] = 1 + (int)image_coord<PT>(g, x[a], a, -1, &c) + (int)image_coord<PT>(g, x[a], a, 1, &c);
-      }
-      cnt = (uint32_t)(opt[0] * opt[1] * opt[2] - 1);
+  const int64_t st = gstride();
+  for (int64_t i0 = gtid(); i0 < n; i0 += 2 * st) {
+    const int64_t i1 = i0 + st;
+    const bool has1 = i1 < n;
+    const int b0 = box_search(s_base, nbox, (uint64_t)i0);
+    const int b1 = has1 ? box_search(s_base, nbox, (uint64_t)i1) : b0;
+    double x0[3], x1[3] = {0.0, 0.0, 0.0};
+    load_pos<PT>(boxes[b0], (uint64_t)i0 - s_base[b0], x0);
+    if (has1) load_pos<PT>(boxes[b1], (uint64_t)i1 - s_base[b1], x1);
+    const uint32_t f0 = ingest_flags<PT>(boxes[b0].g, x0);
+    keep[i0] = f0 & 1u;
+    nimg[i0] = f0 >> 1;
+    if (has1) {
+      const uint32_t f1 = ingest_flags<PT>(boxes[b1].g, x1);
+      keep[i1] = f1 & 1u;
+      nimg[i1] = f1 >> 1;
     }
-    keep[i] = ok ? 1u : 0u;
-    nimg[i] = cnt;
   }
 }
 
@@ -225,16 +244,20 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
     double x[3] = {0.0, 0.0, 0.0};
     uint32_t q0 = 0;
     bool has_img = false;
-    if (i < n && keep[i]) {
+    if (i < n) {
+      // every load of the particle is issued before any is used
       b = box_search(s_base, nbox, (uint64_t)i);
       const BoxDev &bx = boxes[b];
-      load_pos<PT>(bx, (uint64_t)i - bx.in_base, x);
-      const uint32_t pbase = boxd[4 * nbox + b];
-      const uint32_t p = pbase + (keep_scan[i] - boxd[0 * nbox + b]);
-      if (p < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, p, x, (uint32_t)i, keys, vals, ppos);
-      if (bx.g.periodic && nimg[i] != 0) {
-        has_img = true;
-        q0 = pbase + boxd[2 * nbox + b] + (img_scan[i] - boxd[1 * nbox + b]);
+      const uint32_t kp = keep[i], ks = keep_scan[i], is = img_scan[i], ni = nimg[i];
+      load_pos<PT>(bx, (uint64_t)i - s_base[b], x);
+      if (kp) {
+        const uint32_t pbase = boxd[4 * nbox + b];
+        const uint32_t p = pbase + (ks - boxd[0 * nbox + b]);
+        if (p < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, p, x, (uint32_t)i, keys, vals, ppos);
+        if (bx.g.periodic && ni != 0) {
+          has_img = true;
+          q0 = pbase + boxd[2 * nbox + b] + (is - boxd[1 * nbox + b]);
+        }
       }
     }
     unsigned m = __ballot_sync(0xffffffffu, has_img);
@@ -279,8 +302,10 @@ __device__ __forceinline__ uint64_t stored_key(const BoxDev *boxes, const uint64
 
 // Cell-ordered positions, their fine-cell keys (the sort leaves only the
 // order) and run-start flags; flags are 0 past the processed count so that
-// the scan over the capacity counts only real runs.  Lane l compares with
-// lane l-1's key; lane 0 recomputes its predecessor's.
+// the scan over the capacity counts only real runs.  A warp takes two groups
+// of 32 consecutive elements per step (w0 and w0 + stride), with both
+// gathers in flight before either is used.  Lane l compares with lane l-1's
+// key; lane 0 recomputes its predecessor's.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict__ perm,
                                                      const SPos<PT> *__restrict__ ppos,
@@ -295,19 +320,33 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
   load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
   const int lane = threadIdx.x & 31;
-  for (int64_t w0 = gtid() - lane; w0 < cap; w0 += gstride()) {
-    const int64_t i = w0 + lane;
-    uint64_t key = 0;
-    if (i < np) {
-      const SPos<PT> sp = ppos[perm[i]];
-      spos[i] = sp;
-      key = stored_key<PT>(boxes, s_base, nbox, k3all, sp);
-      keys[i] = key;
+  const int64_t st = gstride();
+  for (int64_t w0 = gtid() - lane; w0 < cap; w0 += 2 * st) {
+    int64_t i[2] = {w0 + lane, w0 + st + lane};
+    uint32_t pi[2] = {0u, 0u}, pp[2] = {0u, 0u};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (i[h] < np) pi[h] = perm[i[h]];
+      if (lane == 0 && i[h] > 0 && i[h] < np) pp[h] = perm[i[h] - 1];
     }
-    uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-    if (lane == 0 && i > 0 && i < np)
-      prev = stored_key<PT>(boxes, s_base, nbox, k3all, ppos[perm[i - 1]]);
-    if (i < cap) flag[i] = (i < np && (i == 0 || key != prev)) ? 1u : 0u;
+    SPos<PT> sp[2], sq[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (i[h] < np) sp[h] = ppos[pi[h]];
+      if (lane == 0 && i[h] > 0 && i[h] < np) sq[h] = ppos[pp[h]];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      uint64_t key = 0;
+      if (i[h] < np) {
+        spos[i[h]] = sp[h];
+        key = stored_key<PT>(boxes, s_base, nbox, k3all, sp[h]);
+        keys[i[h]] = key;
+      }
+      uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+      if (lane == 0 && i[h] > 0 && i[h] < np) prev = stored_key<PT>(boxes, s_base, nbox, k3all, sq[h]);
+      if (i[h] < cap) flag[i[h]] = (i[h] < np && (i[h] == 0 || key != prev)) ? 1u : 0u;
+    }
   }
 }
 

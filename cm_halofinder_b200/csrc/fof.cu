@@ -119,6 +119,10 @@ __device__ __forceinline__ void load_pos(const BoxDev &bx, uint64_t li, double x
 
 // Keep flag (bit 0: inside the domain) and image count (bits 1..) of a
 // particle at x.
+// A shift by -L (+L) can only stay in the shell for x within the boundary
+// size of the upper (lower) face: farther in, x -+ L lies beyond the shell by
+// more than the margin, which is far above the rounding of x -+ L to PT, so
+// only particles within the margin are tested exactly.
 template <class PT>
 __device__ __forceinline__ uint32_t ingest_flags(const Geom &g, const double x[3]) {
   if (!in_domain(g, x)) return 0u;
@@ -127,8 +131,11 @@ __device__ __forceinline__ uint32_t ingest_flags(const Geom &g, const double x[3
     int opt[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
+      const double margin = g.boundary + 1e-5 * (fabs(g.lo[a]) + fabs(g.hi[a]) + g.boundary);
       double c;
-      opt[a] = 1 + (int)image_coord<PT>(g, x[a], a, -1, &c) + (int)image_coord<PT>(g, x[a], a, 1, &c);
+      opt[a] = 1;
+      if (g.hi[a] - x[a] <= margin) opt[a] += (int)image_coord<PT>(g, x[a], a, -1, &c);
+      if (x[a] - g.lo[a] <= margin) opt[a] += (int)image_coord<PT>(g, x[a], a, 1, &c);
     }
     cnt = (uint32_t)(opt[0] * opt[1] * opt[2] - 1);
   }
@@ -224,10 +231,10 @@ __device__ __forceinline__ void emit_one(const Geom &g, uint64_t top_base, uint6
 // Processing order of a box: kept originals in input order, then the images
 // grouped by source particle and shift code (sz+1)*9 + (sy+1)*3 + (sx+1)
 // ascending.  Writes beyond the capacity are dropped (the run is then
-// repeated with more room).  A warp walks 32 consecutive particles; the
-// images of each particle that has some are then emitted by the whole warp
-// at once, one shift code per lane, so that the few image particles do not
-// hold the other lanes through a 27-step loop.
+// repeated with more room).  A warp walks 32 consecutive particles; their
+// images are then emitted one per lane (32 at a time), so that image work
+// is proportional to the images, not to the 26 shifts of each particle
+// that has some.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_ingest_emit(
     const BoxDev *__restrict__ boxes, int nbox, int64_t n, uint64_t k3all,
@@ -242,8 +249,7 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
     const int64_t i = w0 + lane;
     int b = 0;
     double x[3] = {0.0, 0.0, 0.0};
-    uint32_t q0 = 0;
-    bool has_img = false;
+    uint32_t q0 = 0, ic = 0, opts = 0;
     if (i < n) {
       // every load of the particle is issued before any is used
       b = box_search(s_base, nbox, (uint64_t)i);
@@ -255,33 +261,69 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
         const uint32_t p = pbase + (ks - boxd[0 * nbox + b]);
         if (p < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, p, x, (uint32_t)i, keys, vals, ppos);
         if (bx.g.periodic && ni != 0) {
-          has_img = true;
+          ic = ni;
           q0 = pbase + boxd[2 * nbox + b] + (is - boxd[1 * nbox + b]);
+          // per axis: whether the -1 / +1 shift stays in the shell
+#pragma unroll
+          for (int a = 0; a < 3; a++) {
+            double c;
+            opts |= (uint32_t)image_coord<PT>(bx.g, x[a], a, -1, &c) << (2 * a);
+            opts |= (uint32_t)image_coord<PT>(bx.g, x[a], a, 1, &c) << (2 * a + 1);
+          }
         }
       }
     }
-    unsigned m = __ballot_sync(0xffffffffu, has_img);
-    while (m) {
-      const int src = __ffs(m) - 1;
-      m &= m - 1;
-      const int64_t si = __shfl_sync(0xffffffffu, i, src);
-      const int sb = __shfl_sync(0xffffffffu, b, src);
-      const uint32_t sq = __shfl_sync(0xffffffffu, q0, src);
-      double sx[3];
+    // The warp's images, one per lane, in (particle, shift code) order: a
+    // particle's images are the product of its per-axis options (-1 | 0 | +1
+    // where the shifted coordinate stays in the shell) without (0, 0, 0),
+    // in ascending code (sz+1)*9 + (sy+1)*3 + (sx+1), so the r-th one is
+    // the r-th (r+1-th past (0, 0, 0)) entry of that product in z, y, x order.
+    uint32_t inc = ic;
 #pragma unroll
-      for (int a = 0; a < 3; a++) sx[a] = __shfl_sync(0xffffffffu, x[a], src);
-      const BoxDev &bx = boxes[sb];
-      const int sh[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
-      bool ok = lane < 27 && lane != 13;
-      double c[3];
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= d) inc += o;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    for (uint32_t m0 = 0; m0 < total; m0 += 32) {
+      const uint32_t m = m0 + (uint32_t)lane;
+      // source lane: the number of lanes whose inclusive count is <= m
+      int own = 0;
 #pragma unroll
-      for (int a = 0; a < 3; a++) {
-        c[a] = sx[a];
-        if (ok && sh[a] != 0) ok = image_coord<PT>(bx.g, sx[a], a, sh[a], &c[a]);
+      for (int st = 16; st >= 1; st >>= 1)
+        if (__shfl_sync(0xffffffffu, inc, own + st - 1) <= m) own += st;
+      const uint32_t o_inc = __shfl_sync(0xffffffffu, inc, own);
+      const uint32_t o_ic = __shfl_sync(0xffffffffu, ic, own);
+      const uint32_t o_opts = __shfl_sync(0xffffffffu, opts, own);
+      const uint32_t o_q0 = __shfl_sync(0xffffffffu, q0, own);
+      const int o_b = __shfl_sync(0xffffffffu, b, own);
+      const int64_t o_i = __shfl_sync(0xffffffffu, i, own);
+      double ox[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) ox[a] = __shfl_sync(0xffffffffu, x[a], own);
+      if (m < total) {
+        const uint32_t r = m - (o_inc - o_ic);
+        int na[3], za[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          za[a] = (int)((o_opts >> (2 * a)) & 1u);
+          na[a] = 1 + za[a] + (int)((o_opts >> (2 * a + 1)) & 1u);
+        }
+        const uint32_t zero = (uint32_t)((za[2] * na[1] + za[1]) * na[0] + za[0]);
+        const uint32_t e = r + (r >= zero ? 1u : 0u);
+        const int sh[3] = {(int)(e % (uint32_t)na[0]) - za[0],
+                           (int)((e / (uint32_t)na[0]) % (uint32_t)na[1]) - za[1],
+                           (int)(e / (uint32_t)(na[0] * na[1])) - za[2]};
+        const BoxDev &bx = boxes[o_b];
+        double c[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          c[a] = ox[a];
+          if (sh[a] != 0) image_coord<PT>(bx.g, ox[a], a, sh[a], &c[a]);
+        }
+        const uint32_t q = o_q0 + r;
+        if (q < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, q, c, (uint32_t)o_i, keys, vals, ppos);
       }
-      const unsigned vm = __ballot_sync(0xffffffffu, ok);
-      const uint32_t q = sq + (uint32_t)__popc(vm & ((1u << lane) - 1u));
-      if (ok && q < np_cap) emit_one<PT>(bx.g, bx.top_base, k3all, q, c, (uint32_t)si, keys, vals, ppos);
     }
   }
 }

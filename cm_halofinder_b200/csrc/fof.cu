@@ -201,7 +201,7 @@ __global__ void k_box_totals(const BoxDev *__restrict__ boxes, int nbox, int64_t
 
 // Fine-cell key of a processed particle at c: (top cell, counted over the
 // run's boxes) * k^3 + the fine cell within it.  c holds the stored (PT)
-// coordinates, so the key can be recomputed from the stored position.
+// coordinates, so the fine cell can be recomputed from the stored position.
 __device__ __forceinline__ uint64_t cell_key(const Geom &g, uint64_t top_base, uint64_t k3all,
                                              const double c[3]) {
   int gi[3];
@@ -332,29 +332,35 @@ __global__ void __launch_bounds__(kT) k_ingest_emit(
 // Runs of equal fine-cell keys.
 // ---------------------------------------------------------------------------
 
-// Fine-cell key of a stored processed particle: its stored coordinates are
-// those the key was emitted from, so the key is the emitted one exactly.
+// Fine cell of a stored processed particle, packed gx | gy << 21 | gz << 42,
+// and its box: the stored coordinates are those its sort key was computed
+// from, so (box, fine cell) is that key's exactly.
 template <class PT>
-__device__ __forceinline__ uint64_t stored_key(const BoxDev *boxes, const uint64_t *s_base,
-                                               int nbox, uint64_t k3all, const SPos<PT> &sp) {
-  const BoxDev &bx = boxes[nbox > 1 ? box_search(s_base, nbox, (uint64_t)sp.src) : 0];
+__device__ __forceinline__ uint64_t stored_cell(const BoxDev *boxes, const uint64_t *s_base,
+                                                int nbox, const SPos<PT> &sp, int *box) {
+  const int b = nbox > 1 ? box_search(s_base, nbox, (uint64_t)sp.src) : 0;
+  const Geom &g = boxes[b].g;
   const double c[3] = {as_d(sp.x), as_d(sp.y), as_d(sp.z)};
-  return cell_key(bx.g, bx.top_base, k3all, c);
+  uint64_t packed = 0;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    packed |= (uint64_t)fine_index(c[a], g.rmin[a], g.inv_h, g.G[a]) << (21 * a);
+  *box = b;
+  return packed;
 }
 
-// Cell-ordered positions, their fine-cell keys (the sort leaves only the
-// order) and run-start flags; flags are 0 past the processed count so that
-// the scan over the capacity counts only real runs.  A warp takes two groups
-// of 32 consecutive elements per step (w0 and w0 + stride), with both
-// gathers in flight before either is used.  Lane l compares with lane l-1's
-// key; lane 0 recomputes its predecessor's.
+// Cell-ordered positions, their packed fine cells (the sort leaves only the
+// order) and run-start flags (a new (box, fine cell) pair); flags are 0 past
+// the processed count so that the scan over the capacity counts only real
+// runs.  A warp takes two groups of 32 consecutive elements per step (w0 and
+// w0 + stride), with both gathers in flight before either is used.  Lane l
+// compares with lane l-1's cell; lane 0 recomputes its predecessor's.
 template <class PT>
 __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict__ perm,
                                                      const SPos<PT> *__restrict__ ppos,
                                                      const BoxDev *__restrict__ boxes, int nbox,
-                                                     uint64_t k3all,
                                                      SPos<PT> *__restrict__ spos,
-                                                     uint64_t *__restrict__ keys,
+                                                     uint64_t *__restrict__ cells,
                                                      uint32_t *__restrict__ flag,
                                                      const DevScal *__restrict__ sc,
                                                      int64_t cap) {
@@ -379,48 +385,47 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
     }
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-      uint64_t key = 0;
+      uint64_t cell = 0;
+      int box = 0;
       if (i[h] < np) {
         spos[i[h]] = sp[h];
-        key = stored_key<PT>(boxes, s_base, nbox, k3all, sp[h]);
-        keys[i[h]] = key;
+        cell = stored_cell<PT>(boxes, s_base, nbox, sp[h], &box);
+        cells[i[h]] = cell;
       }
-      uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-      if (lane == 0 && i[h] > 0 && i[h] < np) prev = stored_key<PT>(boxes, s_base, nbox, k3all, sq[h]);
-      if (i[h] < cap) flag[i[h]] = (i[h] < np && (i[h] == 0 || key != prev)) ? 1u : 0u;
+      uint64_t pcell = __shfl_up_sync(0xffffffffu, cell, 1);
+      int pbox = __shfl_up_sync(0xffffffffu, box, 1);
+      if (lane == 0 && i[h] > 0 && i[h] < np) pcell = stored_cell<PT>(boxes, s_base, nbox, sq[h], &pbox);
+      if (i[h] < cap)
+        flag[i[h]] = (i[h] < np && (i[h] == 0 || cell != pcell || box != pbox)) ? 1u : 0u;
     }
   }
 }
 
-__global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ keys,
+// Run of every processed particle, and per run its first particle, packed
+// fine cell and box.
+template <class PT>
+__global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ cells,
                                              const uint32_t *__restrict__ flag,
                                              const uint32_t *__restrict__ run_scan,
+                                             const SPos<PT> *__restrict__ spos,
                                              const BoxDev *__restrict__ boxes, int nbox,
-                                             uint64_t k3all, DevScal *sc,
+                                             DevScal *sc,
                                              uint32_t *__restrict__ run_of,
                                              uint32_t *__restrict__ run_start,
                                              uint64_t *__restrict__ run_g,
                                              uint16_t *__restrict__ run_box) {
   __shared__ uint64_t s_base[kMaxBoxes];
-  load_bases(boxes, nbox, s_base, true);
+  load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
   const uint32_t R = sc->R;
   for (int64_t i = gtid(); i < np; i += gstride()) {
-    const uint32_t rid = run_scan[i] + flag[i] - 1u;
+    const uint32_t f = flag[i];
+    const uint32_t rid = run_scan[i] + f - 1u;
     run_of[i] = rid;
-    if (flag[i]) {
+    if (f) {
       run_start[rid] = (uint32_t)i;
-      const uint64_t key = keys[i];
-      const uint64_t gtop = key / k3all, sub = key % k3all;
-      const int b = box_search(s_base, nbox, gtop);
-      const Geom &g = boxes[b].g;
-      const uint64_t top = gtop - s_base[b];
-      const int k = g.k;
-      const uint64_t tx = top % g.T[0], ty = (top / g.T[0]) % g.T[1], tz = top / ((uint64_t)g.T[0] * g.T[1]);
-      const uint64_t sx = sub % k, sy = (sub / k) % k, sz = sub / ((uint64_t)k * k);
-      const uint64_t gx = tx * k + sx, gy = ty * k + sy, gz = tz * k + sz;
-      run_g[rid] = gx | (gy << 21) | (gz << 42);
-      run_box[rid] = (uint16_t)b;
+      run_g[rid] = cells[i];
+      run_box[rid] = (uint16_t)(nbox > 1 ? box_search(s_base, nbox, (uint64_t)spos[i].src) : 0);
     }
     if (i == np - 1) run_start[R] = (uint32_t)np;
   }
@@ -1684,7 +1689,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   mark(0);
   // ---- sort ----
   // the sort leaves the indices in cell order in b_vals and no sorted keys:
-  // k_gather_flags recomputes them into b_keys from the positions
+  // k_gather_flags recomputes the fine cells into b_keys from the positions
   radix_order_u64_u32(emit_k, emit_v, odd ? b_keys.as<uint64_t>() : b_keys_alt.as<uint64_t>(),
                       odd ? b_vals.as<uint32_t>() : b_vals_alt.as<uint32_t>(), npc, &sc->np,
                       key_bits, sort_tmp, &c->sort_giveups, s);
@@ -1693,13 +1698,14 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
   uint32_t *run_scan = flag + npc;
   k_gather_flags<PT><<<rg(k_gather_flags<PT>, npc), kT, 0, s>>>(
-      b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>(), boxes, nbox, k3all, b_spos.as<SPos<PT>>(),
+      b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>(), boxes, nbox, b_spos.as<SPos<PT>>(),
       b_keys.as<uint64_t>(), flag, sc, npc);
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s);
-  k_runs<<<rg(k_runs, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan, boxes, nbox, k3all, sc,
-                           run_of, b_run_start.as<uint32_t>(),
-                           run_g, b_run_box.as<uint16_t>());
+  k_runs<PT><<<rg(k_runs<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan,
+                                               b_spos.as<SPos<PT>>(), boxes, nbox, sc, run_of,
+                                               b_run_start.as<uint32_t>(), run_g,
+                                               b_run_box.as<uint16_t>());
   CMH_LAUNCHED();
   if (varlink) {
     if (fp32)

@@ -28,7 +28,7 @@ from ._abi import (CMH_DEVICE, CMH_FLOAT32, CMH_FLOAT64, CMH_FP32_RECHECK, CMH_H
 
 __all__ = [
     "fof", "Plan", "Catalog", "FofConfig", "read_parameterfile", "read_particles",
-    "config_from_run", "write_halos", "write_info",
+    "config_from_run", "write_halos", "write_info", "fof_sampled", "write_subsample",
     "CmhError", "CMH_FP32_RECHECK", "CMH_PLAIN_FP64", "CMH_PROP_INERTIA", "CMH_PROP_DISPERSION",
     "CMH_OUT_UNFORMATTED", "CMH_OUT_PARTICLES", "CMH_OUT_PARTICLE_ID", "halosize",
 ]
@@ -366,8 +366,64 @@ def write_halos(base, task, catalog: Catalog, pos=None, vel=None, ids=None, flag
                                  C.byref(parts) if parts is not None else None, int(flags)))
 
 
-def write_info(base, rp, nhalos_per_task):
+def write_info(base, rp, nhalos_per_task, ninhalo_per_task=None, nouthalo_per_task=None):
+    """Write "<base>.info" (Output_Info); the subsample counts default to 0."""
     L = _abi.lib()
     arr = np.ascontiguousarray(nhalos_per_task, np.int64)
-    _abi.check(L.cmh_write_info(str(base).encode(), C.byref(rp),
-                                arr.ctypes.data_as(C.POINTER(C.c_int64)), len(arr)))
+    cnt = [None if a is None else np.ascontiguousarray(a, np.int64)
+           for a in (ninhalo_per_task, nouthalo_per_task)]
+    ptr = [None if a is None else a.ctypes.data_as(C.POINTER(C.c_int64)) for a in cnt]
+    _abi.check(L.cmh_write_info_sampled(str(base).encode(), C.byref(rp),
+                                        arr.ctypes.data_as(C.POINTER(C.c_int64)), ptr[0],
+                                        ptr[1], len(arr)))
+
+
+def fof_sampled(pos, vel, config: FofConfig, samp_in, samp_out, seed, ids=None,
+                members=False, stream=None, closed_hi=None):
+    """fof() that also draws the SampInHalos / SampOutHalos subsample
+    (FOF.c:205-284): returns (catalog, inhalo, outhalo), the last two the
+    input indices of the kept particles, ascending.  closed_hi (per axis)
+    defaults to the reference's single-rank run: upper faces included when
+    isolated, excluded when periodic."""
+    L = _abi.lib()
+    pos = np.ascontiguousarray(pos)
+    vel = np.ascontiguousarray(vel)
+    if pos.ndim != 2 or pos.shape[1] != 3 or vel.shape != pos.shape:
+        raise ValueError("pos and vel must be (N, 3)")
+    idarr = None if ids is None else np.ascontiguousarray(ids, np.uint64)
+    parts = _abi.Particles(n=pos.shape[0], pos_dtype=_dtype_code(pos), vel_dtype=_dtype_code(vel),
+                           pos=pos.ctypes.data, vel=vel.ctypes.data,
+                           id=None if idarr is None else idarr.ctypes.data, location=CMH_HOST)
+    p = config.to_c()
+    if closed_hi is None:
+        closed_hi = (0, 0, 0) if config.periodic else (1, 1, 1)
+    samp = _abi.Sampling(samp_in=float(samp_in), samp_out=float(samp_out), seed=int(seed),
+                         closed_hi=(C.c_int32 * 3)(*[int(bool(c)) for c in closed_hi]))
+    cat = _abi.Catalog()
+    out = _abi.Sample()
+    _abi.check(L.cmh_fof_run_sampled(C.byref(p), C.byref(parts), C.byref(samp), C.byref(cat),
+                                     int(members), C.byref(out), C.c_void_p(stream or 0)))
+    try:
+        inh = np.ctypeslib.as_array(out.inhalo, shape=(max(out.n_inhalo, 1),))[:out.n_inhalo].copy()
+        outh = np.ctypeslib.as_array(out.outhalo, shape=(max(out.n_outhalo, 1),))[
+            :out.n_outhalo].copy()
+        return _host_catalog(cat), inh, outh
+    finally:
+        L.cmh_catalog_free(C.byref(cat))
+        L.cmh_sample_free(C.byref(out))
+
+
+def write_subsample(base, task, inhalo, pos, vel, idx, ids=None, flags=0):
+    """Write "<base>_inhalo.<task>" (inhalo true) or "<base>_outhalo.<task>"
+    in the layout of Subsample (FOF.c:432-544)."""
+    L = _abi.lib()
+    pos = np.ascontiguousarray(pos)
+    vel = np.ascontiguousarray(vel)
+    idx = np.ascontiguousarray(idx, np.int64)
+    idarr = None if ids is None else np.ascontiguousarray(ids, np.uint64)
+    parts = _abi.Particles(n=pos.shape[0], pos_dtype=_dtype_code(pos), vel_dtype=_dtype_code(vel),
+                           pos=pos.ctypes.data, vel=vel.ctypes.data,
+                           id=None if idarr is None else idarr.ctypes.data, location=CMH_HOST)
+    _abi.check(L.cmh_write_subsample(str(base).encode(), int(task), int(bool(inhalo)),
+                                     C.byref(parts), idx.ctypes.data_as(C.POINTER(C.c_int64)),
+                                     idx.shape[0], int(flags)))

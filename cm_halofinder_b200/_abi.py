@@ -81,6 +81,16 @@ class Tuning(C.Structure):
                 ("tried", C.c_int32)]
 
 
+class Sampling(C.Structure):
+    _fields_ = [("samp_in", C.c_double), ("samp_out", C.c_double), ("seed", C.c_int32),
+                ("closed_hi", C.c_int32 * 3)]
+
+
+class Sample(C.Structure):
+    _fields_ = [("n_inhalo", C.c_int64), ("inhalo", C.POINTER(C.c_int64)),
+                ("n_outhalo", C.c_int64), ("outhalo", C.POINTER(C.c_int64))]
+
+
 class RunParameters(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("Nx", "Ny", "Nz", "Px", "Py", "Pz")] + [
         (k, C.c_double) for k in ("Lxmin", "Lymin", "Lzmin", "Lxmax", "Lymax", "Lzmax")] + [
@@ -124,6 +134,15 @@ SIGNATURES = {
                                   C.POINTER(Particles), C.c_uint32]),
     "cmh_write_info": (C.c_int, [C.c_char_p, C.POINTER(RunParameters), C.POINTER(C.c_int64),
                                  C.c_int32]),
+    "cmh_write_info_sampled": (C.c_int, [C.c_char_p, C.POINTER(RunParameters),
+                                         C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_int64), C.c_int32]),
+    "cmh_fof_run_sampled": (C.c_int, [C.POINTER(FofParams), C.POINTER(Particles),
+                                      C.POINTER(Sampling), C.POINTER(Catalog), C.c_int32,
+                                      C.POINTER(Sample), C.c_void_p]),
+    "cmh_sample_free": (None, [C.POINTER(Sample)]),
+    "cmh_write_subsample": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(Particles),
+                                      C.POINTER(C.c_int64), C.c_int64, C.c_uint32]),
     "cmh_read_particles": (C.c_int, [C.POINTER(RunParameters), C.c_int32, C.c_uint32,
                                      C.POINTER(Particles), C.POINTER(C.c_void_p)]),
     "cmh_particle_store_free": (None, [C.c_void_p]),

@@ -349,17 +349,36 @@ void cmh_catalog_free(cmh_catalog *cat) {
   cat->nhalos = 0;
 }
 
-cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
-                       cmh_catalog *cat, int32_t want_member, void *stream) {
-  CMH_API_BEGIN
+namespace {
+
+// One-shot run of cmh_fof_run / cmh_fof_run_sampled.
+void fof_once(const cmh_fof_params *params, const cmh_particles *parts,
+              const cmh_sampling *sampling, cmh_catalog *cat, int32_t want_member,
+              cmh_sample *sample, void *stream) {
   if (!params || !cat) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "params and catalog are required");
   check_parts(parts);
   memset(cat, 0, sizeof *cat);
+  if (sampling) {
+    if (!sample) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "a sample needs its output");
+    memset(sample, 0, sizeof *sample);
+    if (!(sampling->samp_in >= 0.0 && sampling->samp_in <= 1.0) ||
+        !(sampling->samp_out >= 0.0 && sampling->samp_out <= 1.0))
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "sampling rates must lie in [0, 1]");
+  }
   const int dev = current_device();
   std::unique_ptr<Plan> pl(new Plan(*params, parts->pos_dtype, dev));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cmh_particles dp = *parts;
-  cmh::DevBuf dpos, dvel;
+  // device copies of host inputs, freed on every way out
+  struct Copies {
+    cmh::DevBuf pos, vel, ids;
+    ~Copies() {
+      pos.release();
+      vel.release();
+      ids.release();
+    }
+  } cp;
+  cmh::DevBuf &dpos = cp.pos, &dvel = cp.vel, &dids = cp.ids;
   if (parts->location == CMH_HOST && parts->n > 0) {
     const size_t pb = (size_t)parts->n * 3 * (parts->pos_dtype == CMH_FLOAT64 ? 8 : 4);
     const size_t vb = (size_t)parts->n * 3 * (parts->vel_dtype == CMH_FLOAT64 ? 8 : 4);
@@ -371,17 +390,76 @@ cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
     dp.vel = dvel.p;
     dp.location = CMH_DEVICE;
   }
-  try {
-    pl->run(dp, want_member != 0, s);
-    catalog_to_host(*pl, cat, want_member != 0, 0, s);
-  } catch (...) {
-    dpos.release();
-    dvel.release();
-    throw;
+  if (sampling) {
+    pl->sampling = true;
+    pl->samp_in = sampling->samp_in;
+    pl->samp_out = sampling->samp_out;
+    pl->samp_seed = (uint64_t)(int64_t)sampling->seed;
+    for (int a = 0; a < 3; a++) pl->samp_closed |= (sampling->closed_hi[a] ? 1 : 0) << a;
+    pl->use_graph = false;  // one run: nothing to replay
+    if (parts->id && parts->n > 0) {
+      if (parts->location == CMH_HOST) {
+        dids.ensure((size_t)parts->n * 8);
+        CMH_CUDA(cudaMemcpyAsync(dids.p, parts->id, (size_t)parts->n * 8,
+                                 cudaMemcpyHostToDevice, s));
+        pl->samp_ids = dids.as<uint64_t>();
+      } else {
+        pl->samp_ids = parts->id;
+      }
+    }
   }
-  dpos.release();
-  dvel.release();
+  pl->run(dp, want_member != 0, s);
+  catalog_to_host(*pl, cat, want_member != 0, 0, s);
+  if (sampling) {
+    const int64_t n = parts->n;
+    std::vector<uint8_t> flag((size_t)std::max<int64_t>(n, 1), 0);
+    if (n > 0) {
+      CMH_CUDA(cudaMemcpyAsync(flag.data(), pl->b_samp.p, (size_t)n, cudaMemcpyDeviceToHost, s));
+      CMH_CUDA(cudaStreamSynchronize(s));
+    }
+    int64_t nin = 0, nout = 0;
+    for (int64_t i = 0; i < n; i++) {
+      nin += flag[i] == 1;
+      nout += flag[i] == 2;
+    }
+    sample->inhalo = (int64_t *)malloc(sizeof(int64_t) * (size_t)std::max<int64_t>(nin, 1));
+    sample->outhalo = (int64_t *)malloc(sizeof(int64_t) * (size_t)std::max<int64_t>(nout, 1));
+    if (!sample->inhalo || !sample->outhalo) {
+      free(sample->inhalo);
+      free(sample->outhalo);
+      sample->inhalo = sample->outhalo = nullptr;
+      cmh::fail(CMH_ERR_OUT_OF_MEMORY, "host sample allocation failed");
+    }
+    for (int64_t i = 0; i < n; i++) {
+      if (flag[i] == 1) sample->inhalo[sample->n_inhalo++] = i;
+      else if (flag[i] == 2) sample->outhalo[sample->n_outhalo++] = i;
+    }
+  }
+}
+
+}  // namespace
+
+cmh_status cmh_fof_run(const cmh_fof_params *params, const cmh_particles *parts,
+                       cmh_catalog *cat, int32_t want_member, void *stream) {
+  CMH_API_BEGIN
+  fof_once(params, parts, nullptr, cat, want_member, nullptr, stream);
   CMH_API_END
+}
+
+cmh_status cmh_fof_run_sampled(const cmh_fof_params *params, const cmh_particles *parts,
+                               const cmh_sampling *sampling, cmh_catalog *cat,
+                               int32_t want_member, cmh_sample *sample, void *stream) {
+  CMH_API_BEGIN
+  if (!sampling) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "sampling parameters are required");
+  fof_once(params, parts, sampling, cat, want_member, sample, stream);
+  CMH_API_END
+}
+
+void cmh_sample_free(cmh_sample *sample) {
+  if (!sample) return;
+  free(sample->inhalo);
+  free(sample->outhalo);
+  memset(sample, 0, sizeof *sample);
 }
 
 namespace {

@@ -1234,6 +1234,51 @@ __global__ void __launch_bounds__(kT) k_group_count(const uint32_t *__restrict__
   }
 }
 
+// Subsampling (FOF.c:205-284): every original particle inside its box's
+// domain ([lo, hi) per axis, [lo, hi] on the axes of `closed`) is kept when its uniform is
+// below its group's rate -- samp_in for groups of at least Nphalomin
+// processed particles (FOF.c:202), samp_out for the others.  The uniform is
+// the top 53 bits of SplitMix64's output mix (Steele, Lea & Flood 2014) of
+// key ^ (seed * 0xD1B54A32D192ED03), key = the particle's ID or its input
+// index, so a particle's draw depends on nothing but the seed and itself.
+__device__ __forceinline__ double sample_uniform(uint64_t seed, uint64_t key) {
+  uint64_t z = key ^ (seed * 0xD1B54A32D192ED03ull);
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * 0x1.0p-53;
+}
+
+template <class PT>
+__global__ void __launch_bounds__(kT) k_subsample(
+    const uint32_t *__restrict__ run_of, const uint32_t *__restrict__ parent,
+    const uint32_t *__restrict__ count, const uint32_t *__restrict__ perm,
+    const SPos<PT> *__restrict__ spos, const uint16_t *__restrict__ run_box,
+    const BoxDev *__restrict__ boxes, const uint32_t *__restrict__ boxd, int nbox,
+    const DevScal *__restrict__ sc, const uint64_t *__restrict__ ids, double samp_in,
+    double samp_out, uint64_t seed, int closed, uint8_t *__restrict__ samp) {
+  const int64_t np = sc->np;
+  for (int64_t i = gtid(); i < np; i += gstride()) {
+    const uint32_t run = run_of[i];
+    const int b = run_box[run];
+    if (perm[i] - boxd[4 * nbox + b] >= boxd[2 * nbox + b]) continue;  // an image
+    const Geom &g = boxes[b].g;
+    const SPos<PT> sp = spos[i];
+    const double x[3] = {as_d(sp.x), as_d(sp.y), as_d(sp.z)};
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+      inside &= x[a] >= g.lo[a] && (((closed >> a) & 1) ? x[a] <= g.hi[a] : x[a] < g.hi[a]);
+    if (!inside) continue;
+    const bool in = !((double)count[parent[run]] < g.nphalomin);
+    const double rate = in ? samp_in : samp_out;
+    if (!(rate > 0.0)) continue;
+    const uint64_t key = ids ? ids[sp.src] : (uint64_t)sp.src;
+    if (sample_uniform(seed, key) < rate) samp[sp.src] = in ? 1 : 2;
+  }
+}
+
 // Candidate flags (0 past the run count): roots with at least Nphalomin
 // members (FOF.c:202).
 __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ parent,
@@ -1790,6 +1835,14 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                   b_vals.as<uint32_t>(), sc, b_count.as<uint32_t>(),
                                   b_head.as<uint32_t>());
   CMH_LAUNCHED();
+  if (sampling && n > 0) {
+    CMH_CUDA(cudaMemsetAsync(b_samp.p, 0, (size_t)n, s));
+    k_subsample<PT><<<rg(k_subsample<PT>, npc), kT, 0, s>>>(
+        run_of, b_parent.as<uint32_t>(), b_count.as<uint32_t>(), b_vals.as<uint32_t>(),
+        b_spos.as<SPos<PT>>(), b_run_box.as<uint16_t>(), boxes, boxd, nbox, sc, samp_ids,
+        samp_in, samp_out, samp_seed, samp_closed, b_samp.as<uint8_t>());
+    CMH_LAUNCHED();
+  }
   k_cand_flags<<<rg(k_cand_flags, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(),
                                  b_run_box.as<uint16_t>(), boxes, sc, npc,
                                  b_rtmp1.as<uint32_t>(), extra + 0);
@@ -1964,6 +2017,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   b_count.ensure(npc * 4);
   b_head.ensure(npc * 4);
   b_cand_of_root.ensure(npc * 4);
+  if (sampling) b_samp.ensure((size_t)nn);
   b_cand_root.ensure(ncc * 4);
   b_sums.ensure(ncc * 18 * 8);
   b_warn.ensure(ncc * 4);
@@ -2070,8 +2124,14 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     // the graph stays valid while the inputs, sizes and capacities do
     std::vector<unsigned char> sig(sizeof(BoxDev) * boxes_host.size());
     memcpy(sig.data(), boxes_host.data(), sig.size());
-    const int64_t caps[7] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
-                             (int64_t)dense_min, (int64_t)vel_wait};
+    int64_t samp_bits[3] = {0, 0, 0};
+    memcpy(&samp_bits[0], &samp_in, 8);
+    memcpy(&samp_bits[1], &samp_out, 8);
+    samp_bits[2] = (int64_t)samp_seed ^ ((int64_t)samp_closed << 40);
+    const int64_t caps[10] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
+                              (int64_t)dense_min, (int64_t)vel_wait,
+                              sampling ? samp_bits[0] : -1, samp_bits[1],
+                              samp_bits[2] ^ (int64_t)(uintptr_t)samp_ids};
     sig.insert(sig.end(), (const unsigned char *)caps, (const unsigned char *)caps + sizeof caps);
     // and the workspace addresses the recorded launches use
     each_buf([&](DevBuf &b) {

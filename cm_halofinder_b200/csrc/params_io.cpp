@@ -266,8 +266,10 @@ cmh_status cmh_write_halos(const char *base, int32_t task, const cmh_catalog *ca
   return CMH_OK;
 }
 
-cmh_status cmh_write_info(const char *base, const cmh_run_parameters *rp,
-                          const int64_t *nhalos_per_task, int32_t ntask) {
+cmh_status cmh_write_info_sampled(const char *base, const cmh_run_parameters *rp,
+                                  const int64_t *nhalos_per_task,
+                                  const int64_t *ninhalo_per_task,
+                                  const int64_t *nouthalo_per_task, int32_t ntask) {
   if (!base || !rp || (ntask > 0 && !nhalos_per_task) || ntask != rp->Nx * rp->Ny * rp->Nz) {
     cmh::set_error("info file needs one halo count per task of the Nx*Ny*Nz grid");
     return CMH_ERR_INVALID_ARGUMENT;
@@ -286,10 +288,85 @@ cmh_status cmh_write_info(const char *base, const cmh_run_parameters *rp,
     const double x1 = x0 + ((rp->Lxmax - rp->Lxmin) / (double)Nx);
     const double y1 = y0 + ((rp->Lymax - rp->Lymin) / (double)Ny);
     const double z1 = z0 + ((rp->Lzmax - rp->Lzmin) / (double)Nz);
+    const unsigned nin = ninhalo_per_task ? (unsigned)ninhalo_per_task[i] : 0u;
+    const unsigned nout = nouthalo_per_task ? (unsigned)nouthalo_per_task[i] : 0u;
     fprintf(fp, "%12d %12.6lf %12.6lf %12.6lf %12.6lf %12.6lf %12.6lf %12d %12u %12u\n", i, x0,
-            y0, z0, x1, y1, z1, (int)nhalos_per_task[i], 0u, 0u);
+            y0, z0, x1, y1, z1, (int)nhalos_per_task[i], nin, nout);
   }
   if (fclose(fp) != 0) return io_fail(std::string("I/O error writing ") + fname);
+  return CMH_OK;
+}
+
+cmh_status cmh_write_info(const char *base, const cmh_run_parameters *rp,
+                          const int64_t *nhalos_per_task, int32_t ntask) {
+  return cmh_write_info_sampled(base, rp, nhalos_per_task, nullptr, nullptr, ntask);
+}
+
+cmh_status cmh_write_subsample(const char *base, int32_t task, int32_t in,
+                               const cmh_particles *parts, const int64_t *idx, int64_t n,
+                               uint32_t flags) {
+  const bool unf = flags & CMH_OUT_UNFORMATTED, withid = flags & CMH_OUT_PARTICLE_ID;
+  if (!base || n < 0 || (n > 0 && (!idx || !parts || !parts->pos || !parts->vel ||
+                                    parts->location != CMH_HOST || (withid && !parts->id)))) {
+    cmh::set_error("a subsample needs host positions, velocities (and IDs) and its indices");
+    return CMH_ERR_INVALID_ARGUMENT;
+  }
+  if (n == 0) return CMH_OK;  // FOF.c:457: no file for an empty sample
+  for (int64_t k = 0; k < n; k++)
+    if (idx[k] < 0 || idx[k] >= parts->n) {
+      cmh::set_error("subsample index outside the particles");
+      return CMH_ERR_INVALID_ARGUMENT;
+    }
+  if (n > 0x7fffffffll / 12) {
+    cmh::set_error("subsample larger than a Fortran record");
+    return CMH_ERR_CAPACITY;
+  }
+  auto val = [&](const void *a, int dtype, int64_t i, int c) -> float {
+    return dtype == CMH_FLOAT64 ? (float)((const double *)a)[3 * i + c]
+                                : ((const float *)a)[3 * i + c];
+  };
+  char fname[1100];
+  snprintf(fname, sizeof fname, "%s_%s.%d", base, in ? "inhalo" : "outhalo", task);
+  FILE *fp = fopen(fname, "w");
+  if (!fp) return io_fail(std::string("Unable to open output file ") + fname);
+  bool ok = true;
+  if (unf) {
+    const uint32_t nn = (uint32_t)n;
+    ok &= wr_record(fp, &nn, 4);
+    std::vector<float> block((size_t)n * 3);
+    for (int q = 0; q < 2 && ok; q++) {
+      const void *a = q == 0 ? parts->pos : parts->vel;
+      const int dt = q == 0 ? parts->pos_dtype : parts->vel_dtype;
+      for (int64_t k = 0; k < n; k++)
+        for (int c = 0; c < 3; c++) block[3 * k + c] = val(a, dt, idx[k], c);
+      ok &= wr_record(fp, block.data(), (int32_t)(sizeof(float) * 3 * n));
+    }
+    if (withid && ok) {
+      std::vector<uint64_t> ids((size_t)n);
+      for (int64_t k = 0; k < n; k++) ids[k] = parts->id[idx[k]];
+      if (n > 0x7fffffffll / 8) ok = false;
+      else ok &= wr_record(fp, ids.data(), (int32_t)(sizeof(uint64_t) * n));
+    }
+  } else {
+    for (int64_t k = 0; k < n && ok; k++) {
+      const int64_t i = idx[k];
+      const float pv[6] = {val(parts->pos, parts->pos_dtype, i, 0),
+                           val(parts->pos, parts->pos_dtype, i, 1),
+                           val(parts->pos, parts->pos_dtype, i, 2),
+                           val(parts->vel, parts->vel_dtype, i, 0),
+                           val(parts->vel, parts->vel_dtype, i, 1),
+                           val(parts->vel, parts->vel_dtype, i, 2)};
+      if (withid)
+        ok &= fprintf(fp, "%15llu %15.6f %15.6f %15.6f %15.6f %15.6f %15.6f\n",
+                      (unsigned long long)parts->id[i], pv[0], pv[1], pv[2], pv[3], pv[4],
+                      pv[5]) > 0;
+      else
+        ok &= fprintf(fp, "%15.6f %15.6f %15.6f %15.6f %15.6f %15.6f\n", pv[0], pv[1], pv[2],
+                      pv[3], pv[4], pv[5]) > 0;
+    }
+  }
+  ok &= fclose(fp) == 0;
+  if (!ok) return io_fail(std::string("I/O error writing ") + fname);
   return CMH_OK;
 }
 

@@ -61,6 +61,13 @@ struct Plan : public cmh_plan {
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_side_start = nullptr, ev_vel_ready = nullptr;
   bool vel_wait = false;
+  // subsampling of the run's particles (FOF.c:205-284): rates, seed and the
+  // particle IDs on the device (NULL: the input index is the key)
+  bool sampling = false;
+  double samp_in = 0.0, samp_out = 0.0;
+  uint64_t samp_seed = 0;
+  int samp_closed = 0;  // bit a: the domain includes its upper face on axis a
+  const uint64_t *samp_ids = nullptr;
 
   // workspace
   DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
@@ -71,6 +78,7 @@ struct Plan : public cmh_plan {
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
   DevBuf in_pos, in_vel;  // device copies of host-resident particles
+  DevBuf b_samp;          // per input particle: 0, 1 (kept, in a halo), 2 (kept, outside)
 
   // every workspace buffer, for release and for the graph signature
   template <class F> void each_buf(F f) {
@@ -81,7 +89,7 @@ struct Plan : public cmh_plan {
                      &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
                      &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
                      &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
-                     &in_pos, &in_vel};
+                     &in_pos, &in_vel, &b_samp};
     for (DevBuf *b : all) f(*b);
   }
   void release_workspace();

@@ -8,7 +8,10 @@
  * libcmh_fof, then writes the same files as the reference:
  *   "<OutputFileBase>.<ThisTask>"  the halo catalog (Output_Halos,
  *                                  FOF.c:546-913), with the same -D flags;
- *   "<OutputFileBase>.info"        the task table (Output_Info, FOF.c:917-957).
+ *   "<OutputFileBase>.info"        the task table (Output_Info, FOF.c:917-957);
+ *   "<OutputFileBase>_inhalo.<ThisTask>", "..._outhalo.<ThisTask>"
+ *                                  the subsamples (Subsample, FOF.c:432-544)
+ *                                  when SampInHalos / SampOutHalos > 0.
  * Like the reference, FOF() frees P (FOF.c:333).  Errors go through
  * FatalError (main.c:107-112) after printing the library's message.
  *
@@ -16,9 +19,11 @@
  * OUTPUT_UNFORMATTED, OUTPUT_PARTICLES, INERTIA, DISPERSION) in place of
  * FOF.c, with -I<this repository>/include, and link -lcmh_fof.
  *
- * Not covered: subsampling (SampInHalos / SampOutHalos > 0, FOF.c:205-284)
- * and VARLINK builds (the reference's own VARLINK build does not compile);
- * both stop with an error rather than give a different answer.  The domain is
+ * Subsampling keeps each particle with its group's rate as the reference
+ * does, but draws its own uniforms (a hash of Seed and the particle's ID or
+ * index) instead of GSL RANLUX numbers along the linked rings, so the sample
+ * has the same law, not the same particles.  VARLINK builds stop with an
+ * error (the reference's own VARLINK build does not compile).  The domain is
  * the rank's [rmin, rmax) with its ghost shell already in P, so the library
  * runs non-periodic and keeps the halos whose centre of mass the rank owns,
  * as Checkhalo does (FOF.c:378-430).
@@ -58,11 +63,6 @@ void FOF(void) {
   printf("\nERROR: the B200 FOF() does not support VARLINK builds.\n\n");
   FatalError((char *)"fof_shim.c", __LINE__);
 #endif
-  if (SampInHalos > 0 || SampOutHalos > 0) {
-    printf("\nERROR: the B200 FOF() does not subsample; set SampInHalos and "
-           "SampOutHalos to 0 or below.\n\n");
-    FatalError((char *)"fof_shim.c", __LINE__);
-  }
 
   cmh_fof_params p;
   memset(&p, 0, sizeof p);
@@ -113,8 +113,27 @@ void FOF(void) {
   parts.location = CMH_HOST;
 
   cmh_catalog cat;
-  if (cmh_fof_run(&p, &parts, &cat, /*want_member=*/1, NULL) != CMH_OK)
+  cmh_sample sample;
+  memset(&sample, 0, sizeof sample);
+  const int sampled = SampInHalos > 0 || SampOutHalos > 0;
+  if (sampled) {
+    cmh_sampling sp;
+    memset(&sp, 0, sizeof sp);
+    sp.samp_in = SampInHalos > 0 ? SampInHalos : 0.0;
+    sp.samp_out = SampOutHalos > 0 ? SampOutHalos : 0.0;
+    sp.seed = Seed;
+#ifndef PERIODIC
+    /* the last rank along an axis keeps particles on its upper face
+       (FOF.c:215-229) */
+    sp.closed_hi[0] = Local_nx == Nx - 1;
+    sp.closed_hi[1] = Local_ny == Ny - 1;
+    sp.closed_hi[2] = Local_nz == Nz - 1;
+#endif
+    if (cmh_fof_run_sampled(&p, &parts, &sp, &cat, /*want_member=*/1, &sample, NULL) != CMH_OK)
+      shim_fatal("FoF on the GPU failed", __LINE__);
+  } else if (cmh_fof_run(&p, &parts, &cat, /*want_member=*/1, NULL) != CMH_OK) {
     shim_fatal("FoF on the GPU failed", __LINE__);
+  }
   if (cat.stats.n_edge_warn > 0)
     printf("\nWARNING: Task %d has %lld halo(s) within a linking length of its "
            "boundary region; increase Boundarysize.\n\n",
@@ -136,12 +155,27 @@ void FOF(void) {
 #endif
   if (cmh_write_halos(OutputFileBase, ThisTask, &cat, &parts, flags) != CMH_OK)
     shim_fatal("writing the halo catalog failed", __LINE__);
+  /* the subsamples (FOF.c:303-318); no file for an empty one */
+  const uint32_t sflags = flags & (CMH_OUT_UNFORMATTED | CMH_OUT_PARTICLE_ID);
+  if (SampInHalos > 0 &&
+      cmh_write_subsample(OutputFileBase, ThisTask, 1, &parts, sample.inhalo, sample.n_inhalo,
+                          sflags) != CMH_OK)
+    shim_fatal("writing the in-halo subsample failed", __LINE__);
+  if (SampOutHalos > 0 &&
+      cmh_write_subsample(OutputFileBase, ThisTask, 0, &parts, sample.outhalo, sample.n_outhalo,
+                          sflags) != CMH_OK)
+    shim_fatal("writing the out-of-halo subsample failed", __LINE__);
 
-  /* the info file: every task's halo count to task 0 (FOF.c:926-928) */
+  /* the info file: every task's halo and subsample counts to task 0
+     (FOF.c:926-928) */
   int nh = (int)cat.nhalos;
+  unsigned nsub[2] = {(unsigned)sample.n_inhalo, (unsigned)sample.n_outhalo};
   int *table = (int *)malloc(sizeof(int) * (size_t)NTask);
-  if (!table) FatalError((char *)"fof_shim.c", __LINE__);
+  unsigned *subtab = (unsigned *)malloc(2 * sizeof(unsigned) * (size_t)NTask);
+  if (!table || !subtab) FatalError((char *)"fof_shim.c", __LINE__);
   MPI_Allgather(&nh, 1, MPI_INT, table, 1, MPI_INT, MPI_COMM_WORLD);
+  MPI_Allgather(&nsub[0], 1, MPI_UNSIGNED, subtab, 1, MPI_UNSIGNED, MPI_COMM_WORLD);
+  MPI_Allgather(&nsub[1], 1, MPI_UNSIGNED, subtab + NTask, 1, MPI_UNSIGNED, MPI_COMM_WORLD);
   if (ThisTask == 0) {
     cmh_run_parameters rp;
     memset(&rp, 0, sizeof rp);
@@ -157,15 +191,22 @@ void FOF(void) {
     rp.Lxmax = Lxmax;
     rp.Lymax = Lymax;
     rp.Lzmax = Lzmax;
-    int64_t *counts = (int64_t *)malloc(sizeof(int64_t) * (size_t)NTask);
+    int64_t *counts = (int64_t *)malloc(3 * sizeof(int64_t) * (size_t)NTask);
     if (!counts) FatalError((char *)"fof_shim.c", __LINE__);
-    for (int t = 0; t < NTask; t++) counts[t] = table[t];
-    if (cmh_write_info(OutputFileBase, &rp, counts, NTask) != CMH_OK)
+    for (int t = 0; t < NTask; t++) {
+      counts[t] = table[t];
+      counts[NTask + t] = subtab[t];
+      counts[2 * NTask + t] = subtab[NTask + t];
+    }
+    if (cmh_write_info_sampled(OutputFileBase, &rp, counts, counts + NTask, counts + 2 * NTask,
+                               NTask) != CMH_OK)
       shim_fatal("writing the info file failed", __LINE__);
     free(counts);
   }
+  free(subtab);
   free(table);
 
+  cmh_sample_free(&sample);
   cmh_catalog_free(&cat);
   free(ids);
   free(vel);

@@ -249,6 +249,50 @@ cmh_status cmh_fof_labels_noalloc(const cmh_fof_params *params, const void *pos,
                                   int32_t pos_dtype, int64_t n, uint32_t *label,
                                   void *stream);
 
+/* ---- subsampling (FOF.c:205-284; files by Subsample, FOF.c:432-544) ---- */
+
+/* SampInHalos / SampOutHalos / Seed.  Each original particle inside the
+ * domain ([lo, hi) per axis, [lo, hi] on the axes flagged in closed_hi: the
+ * reference closes the upper face of the last rank along an axis in isolated
+ * builds, FOF.c:215-229) is kept with the rate of its group:
+ * samp_in for groups of at least Nphalomin processed particles (images
+ * included), samp_out for the others.  It is kept when u(Seed, key) < rate,
+ * key = its ID (or its input index without IDs), u = the top 53 bits of
+ * SplitMix64's output mix (Steele, Lea & Flood 2014) of
+ * key ^ (Seed * 0xD1B54A32D192ED03), times 2^-53.  The reference draws GSL
+ * RANLUX numbers along its linked rings (and stops a ring at its first
+ * selected particle outside the domain); neither GSL nor the ring order
+ * exists here, so the sample has the same law, not the same particles. */
+typedef struct cmh_sampling {
+  double samp_in;      /* SampInHalos  (0: none)                              */
+  double samp_out;     /* SampOutHalos (0: none)                              */
+  int32_t seed;        /* Seed                                                */
+  int32_t closed_hi[3];/* 1: the domain includes its upper face on this axis  */
+} cmh_sampling;
+
+typedef struct cmh_sample {
+  int64_t n_inhalo;    /* kept particles of groups with >= Nphalomin members  */
+  int64_t *inhalo;     /* their input indices, ascending (host)               */
+  int64_t n_outhalo;   /* kept particles of the other groups                  */
+  int64_t *outhalo;
+} cmh_sample;
+
+/* cmh_fof_run that also draws the subsample (host arrays in *sample, freed
+ * by cmh_sample_free). */
+cmh_status cmh_fof_run_sampled(const cmh_fof_params *params, const cmh_particles *parts,
+                               const cmh_sampling *sampling, cmh_catalog *cat,
+                               int32_t want_member, cmh_sample *sample, void *stream);
+void cmh_sample_free(cmh_sample *sample);
+
+/* Writes "<base>_inhalo.<task>" (in != 0) or "<base>_outhalo.<task>" in the
+ * layout of Subsample (FOF.c:432-544): unformatted, a count record, then all
+ * positions, all velocities and (CMH_OUT_PARTICLE_ID) all IDs, each one
+ * record; otherwise one "[ID] x y z vx vy vz" line per particle.  No file for
+ * an empty sample.  idx are input indices into the host particles `parts`. */
+cmh_status cmh_write_subsample(const char *base, int32_t task, int32_t in,
+                               const cmh_particles *parts, const int64_t *idx, int64_t n,
+                               uint32_t flags);
+
 /* ---- run-parameter file (startup.c:109-314) ----------------------------- */
 
 /* The reference's tag/value run_parameters file.  Same tags, same rules:
@@ -320,6 +364,12 @@ cmh_status cmh_write_halos(const char *base, int32_t task, const cmh_catalog *ca
 /* Writes "<base>.info" (Output_Info, FOF.c:917-957) for one task grid. */
 cmh_status cmh_write_info(const char *base, const cmh_run_parameters *rp,
                           const int64_t *nhalos_per_task, int32_t ntask);
+/* The same with each task's subsample counts (NSUBSAMPIN, NSUBSAMPOUT);
+ * NULL count arrays write zeros. */
+cmh_status cmh_write_info_sampled(const char *base, const cmh_run_parameters *rp,
+                                  const int64_t *nhalos_per_task,
+                                  const int64_t *ninhalo_per_task,
+                                  const int64_t *nouthalo_per_task, int32_t ntask);
 
 #ifdef __cplusplus
 }

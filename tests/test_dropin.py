@@ -107,17 +107,44 @@ def test_dropin_no_halos_writes_no_catalog(tmp_path):
         assert f2.read() == f1.read()
 
 
-def test_dropin_rejects_subsampling(tmp_path):
-    """Subsampling is not offered: the program stops through FatalError
-    before any device work, instead of writing a different catalog."""
-    exe = _exe("cmh_dropin_f32")
-    w = synth.config2(seed=405, scale=3000 / 256 ** 3)
+@pytest.mark.gpu
+def test_dropin_subsamples(tmp_path):
+    """SampInHalos / SampOutHalos > 0: the drop-in writes the same catalog
+    as the reference (which runs without sampling here: its GSL draw is not
+    available), "<base>_inhalo.0" / "_outhalo.0" in Subsample's unformatted
+    layout holding exactly the particles the library's own sampled run keeps
+    on the same input, and the counts in the info file."""
+    from cm_halofinder_b200 import FofConfig, fof_sampled
+    from tests.subsample_ref import read_unformatted
+    w = synth.make_box(20000, 60.0, 400, 405, nphalomin=5, boundary=3.0)
     params = _prepare(w, str(tmp_path))
-    text = open(params["gpu"]).read().replace("SampInHalos -1", "SampInHalos 0.5")
+    text = open(params["gpu"]).read()
+    text = text.replace("SampInHalos -1", "SampInHalos 0.3").replace(
+        "SampOutHalos -1", "SampOutHalos 0.05").replace("Seed 1", "Seed 41")
     open(params["gpu"], "w").write(text)
-    r = subprocess.run([exe, params["gpu"]], capture_output=True, text=True, timeout=120)
-    assert r.returncode == 1
-    assert "does not subsample" in r.stdout
+    _run(os.path.join(reference.REF_DIR, "cmh_ref_f32"), params["ref"])
+    _run(_exe("cmh_dropin_f32"), params["gpu"])
+    # the catalog is the reference's; the info file differs only in the counts
+    ref = reference.read_catalog(os.path.join(tmp_path, "ref.0"), HALOSIZE)
+    got = reference.read_catalog(os.path.join(tmp_path, "gpu.0"), HALOSIZE)
+    assert len(got) == len(ref) > 5
+    for h, g in zip(ref, got):
+        np.testing.assert_array_equal(np.sort(g["ids"]), np.sort(h["ids"]))
+    # the same draw through the library on the program's P[] (the pre-ghosted
+    # processing array, run isolated on [lo, hi] with the upper faces closed)
+    src, ppos, _ = cpu.build_proc(w)
+    ids = np.asarray(src, np.uint64)
+    cfg = FofConfig(lo=w.lo, hi=w.hi, boundary=w.boundary, linklength=w.linklength,
+                    nphalomin=w.nphalomin, periodic=False)
+    _, inh, outh = fof_sampled(ppos, w.vel[src], cfg, 0.3, 0.05, 41, ids=ids)
+    for name, idx in (("inhalo", inh), ("outhalo", outh)):
+        p, v, i = read_unformatted(os.path.join(tmp_path, f"gpu_{name}.0"))
+        np.testing.assert_array_equal(i, ids[idx])
+        np.testing.assert_array_equal(p, ppos[idx])
+        np.testing.assert_array_equal(v, w.vel[src][idx])
+    rows = open(os.path.join(tmp_path, "gpu.info")).read().splitlines()[1].split()
+    assert rows[7:] == [str(len(got)), str(len(inh)), str(len(outh))]
+    assert len(inh) > 100 and len(outh) > 100
 
 
 def test_dropin_without_gpu_reports_the_library_error(tmp_path):

@@ -145,9 +145,11 @@ def stage_bytes(st, pos_bytes):
     design (processed particles npr, fine cells R, position record rec)."""
     n, npr, R = st["n_in"], st["n_proc"], st["n_cells"]
     bits = st["key_bits"]
-    passes = (bits + 7) // 8
-    # passes reading 64-bit keys; the last of them writes 32-bit key words
-    wide = min(passes, max(1, -(-(bits - 32) // 8)))
+    # passes reading 64-bit keys (the last of them writes 32-bit key words),
+    # then 32-bit passes, 9-bit digits where that saves a pass
+    wide = min((bits + 7) // 8, max(1, -(-(bits - 32) // 8)))
+    rest = max(0, bits - 8 * wide)
+    passes = wide + min((rest + 7) // 8, (rest + 8) // 9)
     rec = 16 if pos_bytes == 4 else 32
     return {
         "ingest": 2 * 3 * pos_bytes * n + npr * (8 + 4 + rec),

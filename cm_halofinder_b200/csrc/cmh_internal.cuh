@@ -66,9 +66,12 @@ struct DevBuf {
 
 // ---- scan.cu ---------------------------------------------------------------
 // Exclusive prefix sum of n uint32 values; `total` (device, may be null)
-// receives the sum.  Scratch is taken from `tmp` (grown as needed).
+// receives the sum.  Scratch is taken from `tmp` (grown as needed).  With
+// `n_dev` (device) only the first min(n, *n_dev) entries are read and
+// written; n sizes the launches.
 void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n,
-                        uint32_t *total, DevBuf &tmp, cudaStream_t s);
+                        uint32_t *total, DevBuf &tmp, cudaStream_t s,
+                        const uint32_t *n_dev = nullptr);
 
 // ---- radix_sort.cu -----------------------------------------------------------
 // Stable LSD radix sort of (key u64, value u32) pairs on the low `bits` key
@@ -85,9 +88,10 @@ void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s,
                         bool copy_back = true);
 // The values of the same sort, in key order, without the sorted keys: both
-// key buffers end as scratch (the later passes move 32-bit key words), and
-// the values end in vals_alt after an odd number of 8-bit passes, else in
-// vals.
+// key buffers end as scratch (the later passes move 32-bit key words, with
+// 9-bit digits where that saves a pass), and the values end in vals_alt
+// after an odd number of passes (radix_order_passes), else in vals.
+int radix_order_passes(int bits);
 void radix_order_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                          uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
                          DevBuf &tmp, unsigned int *giveups, cudaStream_t s);

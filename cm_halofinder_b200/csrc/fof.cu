@@ -350,9 +350,8 @@ __device__ __forceinline__ uint64_t stored_cell(const BoxDev *boxes, const uint6
 }
 
 // Cell-ordered positions, their packed fine cells (the sort leaves only the
-// order) and run-start flags (a new (box, fine cell) pair); flags are 0 past
-// the processed count so that the scan over the capacity counts only real
-// runs.  A warp takes two groups of 32 consecutive elements per step (w0 and
+// order) and run-start flags (a new (box, fine cell) pair) of the processed
+// particles (their scan reads no more).  A warp takes two groups of 32 consecutive elements per step (w0 and
 // w0 + stride), with both gathers in flight before either is used.  Lane l
 // compares with lane l-1's cell; lane 0 recomputes its predecessor's.
 template <class PT>
@@ -369,7 +368,7 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
   const int64_t np = sc->np;
   const int lane = threadIdx.x & 31;
   const int64_t st = gstride();
-  for (int64_t w0 = gtid() - lane; w0 < cap; w0 += 2 * st) {
+  for (int64_t w0 = gtid() - lane; w0 < np; w0 += 2 * st) {
     int64_t i[2] = {w0 + lane, w0 + st + lane};
     uint32_t pi[2] = {0u, 0u}, pp[2] = {0u, 0u};
 #pragma unroll
@@ -395,8 +394,7 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
       uint64_t pcell = __shfl_up_sync(0xffffffffu, cell, 1);
       int pbox = __shfl_up_sync(0xffffffffu, box, 1);
       if (lane == 0 && i[h] > 0 && i[h] < np) pcell = stored_cell<PT>(boxes, s_base, nbox, sq[h], &pbox);
-      if (i[h] < cap)
-        flag[i[h]] = (i[h] < np && (i[h] == 0 || cell != pcell || box != pbox)) ? 1u : 0u;
+      if (i[h] < np) flag[i[h]] = (i[h] == 0 || cell != pcell || box != pbox) ? 1u : 0u;
     }
   }
 }
@@ -488,7 +486,7 @@ __global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ 
 }
 
 // 1 on the first fine cell of a top cell with more than dense_min fine cells
-// (0 past the run count).
+// (the first R entries: their scan reads no more).
 __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__ run_g,
                                                     const uint16_t *__restrict__ run_box,
                                                     const BoxDev *__restrict__ boxes,
@@ -497,14 +495,10 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
                                                     uint32_t dense_min,
                                                     uint32_t *__restrict__ flag) {
   const uint32_t R = sc->R;
-  for (int64_t r = gtid(); r < cap; r += gstride()) {
-    uint32_t f = 0;
-    if (r < R) {
-      const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
-      const uint2 tr = top_range[t];
-      f = (tr.x == (uint32_t)r && tr.y - tr.x > dense_min) ? 1u : 0u;
-    }
-    flag[r] = f;
+  for (int64_t r = gtid(); r < (int64_t)R; r += gstride()) {
+    const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
+    const uint2 tr = top_range[t];
+    flag[r] = (tr.x == (uint32_t)r && tr.y - tr.x > dense_min) ? 1u : 0u;
   }
 }
 
@@ -1279,7 +1273,7 @@ __global__ void __launch_bounds__(kT) k_subsample(
   }
 }
 
-// Candidate flags (0 past the run count): roots with at least Nphalomin
+// Candidate flags of the R fine cells: roots with at least Nphalomin
 // members (FOF.c:202).
 __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ parent,
                                                    const uint32_t *__restrict__ count,
@@ -1290,14 +1284,11 @@ __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ 
                                                    unsigned long long *ngroups) {
   const uint32_t R = sc->R;
   unsigned long long roots = 0;
-  for (int64_t r = gtid(); r < cap; r += gstride()) {
-    uint32_t f = 0;
-    if (r < R) {
-      const bool root = parent[r] == (uint32_t)r;
-      roots += root;
-      f = (root && !((double)count[r] < boxes[run_box[r]].g.nphalomin)) ? 1u : 0u;
-    }
-    flag[r] = f;
+  // (the scan of the flags reads the first R only)
+  for (int64_t r = gtid(); r < (int64_t)R; r += gstride()) {
+    const bool root = parent[r] == (uint32_t)r;
+    roots += root;
+    flag[r] = (root && !((double)count[r] < boxes[run_box[r]].g.nphalomin)) ? 1u : 0u;
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) roots += __shfl_down_sync(0xffffffffu, roots, d);
@@ -1709,7 +1700,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   // ---- ingest ----
   // keys and indices are emitted where an odd number of sort passes starts,
   // so that the last pass leaves the indices in b_vals
-  const bool odd = ((key_bits + 7) / 8) % 2 == 1;
+  const bool odd = radix_order_passes(key_bits) % 2 == 1;
   uint64_t *emit_k = odd ? b_keys_alt.as<uint64_t>() : b_keys.as<uint64_t>();
   uint32_t *emit_v = odd ? b_vals_alt.as<uint32_t>() : b_vals.as<uint32_t>();
   if (n > 0) {
@@ -1746,7 +1737,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
       b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>(), boxes, nbox, b_spos.as<SPos<PT>>(),
       b_keys.as<uint64_t>(), flag, sc, npc);
   CMH_LAUNCHED();
-  exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s);
+  exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s, &sc->np);
   k_runs<PT><<<rg(k_runs<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan,
                                                b_spos.as<SPos<PT>>(), boxes, nbox, sc, run_of,
                                                b_run_start.as<uint32_t>(), run_g,
@@ -1772,7 +1763,8 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                   npc, b_top_range.as<uint2>(),
                                   dense_min, b_rtmp1.as<uint32_t>());
   CMH_LAUNCHED();
-  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s);
+  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s,
+                     &sc->R);
   k_clamp_dense<<<1, 32, 0, s>>>(sc, (uint32_t)nd_cap);
   CMH_LAUNCHED();
   k_dense_slots<<<rg(k_dense_slots, npc), kT, 0, s>>>(
@@ -1847,7 +1839,8 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                  b_run_box.as<uint16_t>(), boxes, sc, npc,
                                  b_rtmp1.as<uint32_t>(), extra + 0);
   CMH_LAUNCHED();
-  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nc, scan_tmp, s);
+  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nc, scan_tmp, s,
+                     &sc->R);
   k_cand_list<<<rg(k_cand_list, npc), kT, 0, s>>>(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), sc,
                                 b_cand_of_root.as<uint32_t>(), b_cand_root.as<uint32_t>());
   CMH_LAUNCHED();

@@ -56,9 +56,17 @@ __device__ __forceinline__ void load_items(const uint32_t *in, int64_t n, int64_
   }
 }
 
+// n_dev (device, may be null): the count actually scanned, at most n; the
+// entries past it are taken as 0 and not read or written.
+__device__ __forceinline__ int64_t live_count(int64_t n, const uint32_t *n_dev) {
+  return n_dev ? min(n, (int64_t)*n_dev) : n;
+}
+
 __global__ void __launch_bounds__(kThreads) k_tile_reduce(const uint32_t *in, int64_t n,
+                                                          const uint32_t *n_dev,
                                                           uint32_t *sums) {
   __shared__ uint32_t tot;
+  n = live_count(n, n_dev);
   uint32_t x[kIPT];
   load_items(in, n, (int64_t)blockIdx.x * kTile, x);
   uint32_t s = 0;
@@ -69,9 +77,11 @@ __global__ void __launch_bounds__(kThreads) k_tile_reduce(const uint32_t *in, in
 }
 
 __global__ void __launch_bounds__(kThreads) k_tile_scan(const uint32_t *in, uint32_t *out,
-                                                        int64_t n, const uint32_t *offsets,
+                                                        int64_t n, const uint32_t *n_dev,
+                                                        const uint32_t *offsets,
                                                         uint32_t *total) {
   __shared__ uint32_t tot;
+  n = live_count(n, n_dev);
   uint32_t x[kIPT];
   const int64_t base = (int64_t)blockIdx.x * kTile;
   load_items(in, n, base, x);
@@ -102,27 +112,27 @@ __global__ void __launch_bounds__(kThreads) k_tile_scan(const uint32_t *in, uint
     *total = (offsets ? offsets[blockIdx.x] : 0u) + tot;
 }
 
-void scan_level(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *total,
-                uint32_t *scratch, cudaStream_t s) {
+void scan_level(const uint32_t *in, uint32_t *out, int64_t n, const uint32_t *n_dev,
+                uint32_t *total, uint32_t *scratch, cudaStream_t s) {
   const int64_t nt = (n + kTile - 1) / kTile;
   if (nt == 1) {
-    k_tile_scan<<<1, kThreads, 0, s>>>(in, out, n, nullptr, total);
+    k_tile_scan<<<1, kThreads, 0, s>>>(in, out, n, n_dev, nullptr, total);
     CMH_LAUNCHED();
     return;
   }
   uint32_t *sums = scratch;
   uint32_t *sums_scan = scratch + nt;
-  k_tile_reduce<<<(unsigned)nt, kThreads, 0, s>>>(in, n, sums);
+  k_tile_reduce<<<(unsigned)nt, kThreads, 0, s>>>(in, n, n_dev, sums);
   CMH_LAUNCHED();
-  scan_level(sums, sums_scan, nt, nullptr, scratch + 2 * nt, s);
-  k_tile_scan<<<(unsigned)nt, kThreads, 0, s>>>(in, out, n, sums_scan, total);
+  scan_level(sums, sums_scan, nt, nullptr, nullptr, scratch + 2 * nt, s);
+  k_tile_scan<<<(unsigned)nt, kThreads, 0, s>>>(in, out, n, n_dev, sums_scan, total);
   CMH_LAUNCHED();
 }
 
 }  // namespace
 
 void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *total,
-                        DevBuf &tmp, cudaStream_t s) {
+                        DevBuf &tmp, cudaStream_t s, const uint32_t *n_dev) {
   if (n <= 0) {
     if (total) CMH_CUDA(cudaMemsetAsync(total, 0, sizeof(uint32_t), s));
     return;
@@ -133,7 +143,7 @@ void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *
     need += 2 * m;
   }
   tmp.ensure((size_t)(need + 16) * sizeof(uint32_t));
-  scan_level(in, out, n, total, tmp.as<uint32_t>(), s);
+  scan_level(in, out, n, n_dev, total, tmp.as<uint32_t>(), s);
 }
 
 }  // namespace cmh

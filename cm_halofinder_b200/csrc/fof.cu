@@ -361,8 +361,7 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
                                                      SPos<PT> *__restrict__ spos,
                                                      uint64_t *__restrict__ cells,
                                                      uint32_t *__restrict__ flag,
-                                                     const DevScal *__restrict__ sc,
-                                                     int64_t cap) {
+                                                     const DevScal *__restrict__ sc) {
   __shared__ uint64_t s_base[kMaxBoxes];
   load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
@@ -490,7 +489,7 @@ __global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ 
 __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__ run_g,
                                                     const uint16_t *__restrict__ run_box,
                                                     const BoxDev *__restrict__ boxes,
-                                                    const DevScal *__restrict__ sc, int64_t cap,
+                                                    const DevScal *__restrict__ sc,
                                                     const uint2 *__restrict__ top_range,
                                                     uint32_t dense_min,
                                                     uint32_t *__restrict__ flag) {
@@ -1279,7 +1278,7 @@ __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ 
                                                    const uint32_t *__restrict__ count,
                                                    const uint16_t *__restrict__ run_box,
                                                    const BoxDev *__restrict__ boxes,
-                                                   const DevScal *__restrict__ sc, int64_t cap,
+                                                   const DevScal *__restrict__ sc,
                                                    uint32_t *__restrict__ flag,
                                                    unsigned long long *ngroups) {
   const uint32_t R = sc->R;
@@ -1735,7 +1734,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   uint32_t *run_scan = flag + npc;
   k_gather_flags<PT><<<rg(k_gather_flags<PT>, npc), kT, 0, s>>>(
       b_vals.as<uint32_t>(), b_ppos.as<SPos<PT>>(), boxes, nbox, b_spos.as<SPos<PT>>(),
-      b_keys.as<uint64_t>(), flag, sc, npc);
+      b_keys.as<uint64_t>(), flag, sc);
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s, &sc->np);
   k_runs<PT><<<rg(k_runs<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan,
@@ -1760,8 +1759,8 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                  b_top_range.as<uint32_t>());
   CMH_LAUNCHED();
   k_dense_flags<<<rg(k_dense_flags, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                  npc, b_top_range.as<uint2>(),
-                                  dense_min, b_rtmp1.as<uint32_t>());
+                                  b_top_range.as<uint2>(), dense_min,
+                                  b_rtmp1.as<uint32_t>());
   CMH_LAUNCHED();
   exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s,
                      &sc->R);
@@ -1836,7 +1835,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_LAUNCHED();
   }
   k_cand_flags<<<rg(k_cand_flags, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(),
-                                 b_run_box.as<uint16_t>(), boxes, sc, npc,
+                                 b_run_box.as<uint16_t>(), boxes, sc,
                                  b_rtmp1.as<uint32_t>(), extra + 0);
   CMH_LAUNCHED();
   exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nc, scan_tmp, s,

@@ -135,7 +135,7 @@ BEFRIEND_DRAM_PER_PROC = 444.50e6 / 8971801
 KERNELS = {
     "befriend": "befriending stage: k_befriend_dense + k_befriend_simple + 2 x k_befriend "
                 "(near, far) + 2 x k_compress",
-    "sort": "radix sort: k_rs_upfront + 5 x k_rs_scatter",
+    "sort": "radix sort: k_rs_upfront + one k_rs_scatter per digit pass (4 for 34-bit keys)",
     "ingest": "k_ingest_count + 2 scans + k_ingest_emit",
 }
 
@@ -546,8 +546,12 @@ def run_reference(args):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": f"{args.config} (sampled sub-domains)"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        # MEMORY_MODE: float coordinate differences, double d^2 (FOF.c:351-357)
+        "dtype": "f32+f64" if w.pos.dtype == np.float32 else "f64",
+        "data": "synthetic (seeded Plummer clumps + uniform background)",
+        "config": {"workload": describe(args, w, w.pos.dtype, w.n),
+                   "reference_run": "sampled sub-domains of the box (see cpu_baseline.sample)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

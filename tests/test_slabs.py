@@ -136,7 +136,7 @@ def _rank_main(rank, world, port, grid, periodic, out):
 
 
 @pytest.mark.parametrize("grid,periodic", [((2, 1, 1), True), ((2, 2, 1), True),
-                                           ((2, 2, 1), False)])
+                                           ((3, 1, 1), True), ((2, 2, 1), False)])
 def test_gloo_ranks_find_the_single_box_catalog(grid, periodic):
     from oracle import cpu
     world = grid[0] * grid[1] * grid[2]

@@ -15,6 +15,9 @@
 // Sharing: every call on a device uses the same array.  Each call clears what
 // must start empty before use, but two calls whose work overlaps on the GPU
 // (for instance on two streams) race on the array and give wrong labels.
+#include <cuda.h>
+
+#include <cmath>
 #include <mutex>
 
 #include "cmh_internal.cuh"
@@ -37,24 +40,57 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc;
 
-// Host-side address of g_noalloc on each device, looked up once per device
-// with that device current.  In host code the symbol itself is only a
-// stand-in, never a device address.
+// Host-side address of g_noalloc on each device, looked up with that device
+// current.  In host code the symbol itself is only a stand-in, never a device
+// address.  The lookup is redone only when the device's context changed (a
+// cudaDeviceReset followed by new work loads the module again, and the array
+// may then sit elsewhere); the context is told apart by its ID, which the
+// driver never reuses within a process.
 std::mutex g_addr_mutex;
-NoAllocScratch *g_addr[128] = {};
+struct ScratchAddr {
+  NoAllocScratch *p = nullptr;
+  unsigned long long ctx_id = 0;
+};
+ScratchAddr g_addr[128];
+
+// ID of the calling thread's current context, 0 when none is current.
+unsigned long long current_context_id() {
+  typedef CUresult(CUDAAPI * CtxGetCurrent)(CUcontext *);
+  typedef CUresult(CUDAAPI * CtxGetId)(CUcontext, unsigned long long *);
+  static CtxGetCurrent get_current = nullptr;
+  static CtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void **)&get_current, cudaEnableDefault,
+                                &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void **)&get_id, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 NoAllocScratch *scratch_on(int device) {
   std::lock_guard<std::mutex> lock(g_addr_mutex);
   if (device < 0 || device >= 128) fail(CMH_ERR_INVALID_ARGUMENT, "device index out of range");
-  if (!g_addr[device]) {
+  ScratchAddr &a = g_addr[device];
+  const unsigned long long id = current_context_id();
+  if (!a.p || id == 0 || id != a.ctx_id) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc);
     if (e != cudaSuccess || !p)
       fail(CMH_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
                              cudaGetErrorString(e));
-    g_addr[device] = static_cast<NoAllocScratch *>(p);
+    a.p = static_cast<NoAllocScratch *>(p);
+    a.ctx_id = current_context_id();  // the lookup made the primary context current
   }
-  return g_addr[device];
+  return a.p;
 }
 
 struct NaGrid {
@@ -165,24 +201,33 @@ extern "C" cmh_status cmh_fof_labels_noalloc(const cmh_fof_params *params, const
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
     NaGrid g{};
-    double vol = 1.0;
+    double ext[3];
     for (int a = 0; a < 3; a++) {
       g.rmin[a] = params->lo[a] - params->boundary;
       g.rmax[a] = params->hi[a] + params->boundary;
-      if (!(g.rmax[a] > g.rmin[a])) fail(CMH_ERR_INVALID_ARGUMENT, "empty domain");
-      vol *= g.rmax[a] - g.rmin[a];
+      ext[a] = g.rmax[a] - g.rmin[a];
+      if (!(ext[a] > 0) || !std::isfinite(ext[a]))
+        fail(CMH_ERR_INVALID_ARGUMENT, "empty or unbounded domain");
     }
     g.linksq = params->linklength * params->linklength;
-    g.lc = params->linklength;  // cells no smaller than the linking length
-    for (;;) {
-      int64_t total = 1;
+    // Cells no smaller than the linking length (so the 27-cell scan sees
+    // every linked pair), and at least as large as the side that spreads the
+    // padded domain over kMaxCells cells.  Counts are formed in double and
+    // checked before any conversion to int.
+    g.lc = std::max(params->linklength, std::cbrt(ext[0] * ext[1] * ext[2] / (double)kMaxCells));
+    double cells[3] = {0, 0, 0};
+    for (int it = 0;; it++) {
+      double total = 1.0;
       for (int a = 0; a < 3; a++) {
-        g.nc[a] = (int)((g.rmax[a] - g.rmin[a]) / g.lc) + 1;
-        total *= g.nc[a];
+        cells[a] = std::floor(ext[a] / g.lc) + 1.0;
+        total *= cells[a];
       }
-      if (total <= kMaxCells) break;
+      if (total <= (double)kMaxCells) break;
+      if (it >= 64 || !std::isfinite(g.lc))
+        fail(CMH_ERR_INVALID_ARGUMENT, "no cell grid of at most 2^18 cells covers the domain");
       g.lc *= 1.25;
     }
+    for (int a = 0; a < 3; a++) g.nc[a] = (int)cells[a];  // each <= kMaxCells
     int64_t ncell = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
     const int ni = (int)n;
     const unsigned grid = grid_for(ncell > n ? ncell : n, kThreads, 4);

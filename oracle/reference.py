@@ -23,7 +23,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference"
+# The reference tree (its src_v2/ sources) comes from the environment; unset,
+# nothing here is rebuilt and the prebuilt binaries in _ref/ are used as found.
+REF_SRC = os.environ.get("CMH_REFERENCE") or None
 
 
 def available(binary="cmh_ref_f32"):
@@ -32,8 +34,8 @@ def available(binary="cmh_ref_f32"):
 
 def build():
     """Compile the reference binaries (needs the reference sources)."""
-    if not os.path.isdir(REF_SRC):
-        raise FileNotFoundError("reference sources are not present")
+    if not REF_SRC or not os.path.isdir(REF_SRC):
+        raise FileNotFoundError("reference sources are not present (set CMH_REFERENCE)")
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
 
 

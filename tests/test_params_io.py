@@ -85,10 +85,13 @@ def test_varlink_tags(tmp_path, native_lib):
     assert rp.Omega == 0.25 and rp.Origin_x == 1.5          # float, not the INT typo
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/files/run_parameters.dat"),
-                    reason="reference sources not present")
+REF_EXAMPLE = os.path.join(os.environ.get("CMH_REFERENCE", ""), "files", "run_parameters.dat")
+
+
+@pytest.mark.skipif(not os.environ.get("CMH_REFERENCE") or not os.path.exists(REF_EXAMPLE),
+                    reason="reference sources not given (CMH_REFERENCE)")
 def test_reference_example_file_parses(native_lib):
-    rp = cmh.read_parameterfile("/root/reference/files/run_parameters.dat")
+    rp = cmh.read_parameterfile(REF_EXAMPLE)
     assert (rp.Nx, rp.Ny, rp.Nz, rp.Px) == (2, 2, 2, 256)
     assert rp.Linklength == 0.625 and rp.Boundarysize == 35
 

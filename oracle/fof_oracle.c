@@ -6,8 +6,11 @@
 #include "fof_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
+#include <stdatomic.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 int cmh_oracle_halosize(int props) {
   int hs = 7;                 /* FOF.c:574 */
@@ -157,7 +160,8 @@ double cmh_oracle_cell_linksq(const cmh_oracle_params *p, const double *rmin_buf
 /* FoF (FOF.c:23-161 with union-find in place of Befriend's ring splice).  */
 /* ---------------------------------------------------------------------- */
 
-static int64_t uf_find(int64_t *parent, int64_t x) {
+/* Union-find over cell-ordered slots (see below), hook to the lower slot. */
+static uint32_t uf_find(uint32_t *parent, uint32_t x) {
   while (parent[x] != x) {
     parent[x] = parent[parent[x]];
     x = parent[x];
@@ -165,12 +169,123 @@ static int64_t uf_find(int64_t *parent, int64_t x) {
   return x;
 }
 
-static void uf_union(int64_t *parent, int64_t a, int64_t b) {
-  a = uf_find(parent, a);
-  b = uf_find(parent, b);
-  if (a == b) return;
-  if (a < b) parent[b] = a;
-  else parent[a] = b;
+/* Joins the components of roots a != b; returns the new root. */
+static uint32_t uf_hook(uint32_t *parent, uint32_t a, uint32_t b) {
+  if (a < b) { parent[b] = a; return a; }
+  parent[a] = b;
+  return b;
+}
+
+typedef struct { uint32_t a, b; } link_t;
+
+/* What the cell scan shares between threads (read-only) and keeps per thread. */
+typedef struct {
+  const cmh_oracle_params *p;
+  int dbl, nc[3];
+  const int64_t *cstart;          /* first slot of every cell, ncell + 1 */
+  const void *spos;               /* positions in slot order */
+  double rmin_buff[3], lcell[3], linksq;
+  _Atomic int64_t *next_row;      /* rows (iz, iy) handed out one at a time */
+} scan_shared;
+
+typedef struct {
+  const scan_shared *sh;
+  uint32_t *parent;               /* this thread's union-find over all slots */
+  link_t *links;                  /* the joins it made: a spanning forest of its links */
+  int64_t nlinks, caplinks, ntests;
+  int err;
+} scan_thread;
+
+static void add_link(scan_thread *t, uint32_t a, uint32_t b) {
+  if (t->nlinks == t->caplinks) {
+    int64_t cap = t->caplinks ? 2 * t->caplinks : 4096;
+    link_t *nl = (link_t *)realloc(t->links, sizeof(link_t) * (size_t)cap);
+    if (!nl) { t->err = 1; return; }
+    t->links = nl;
+    t->caplinks = cap;
+  }
+  t->links[t->nlinks].a = a;
+  t->links[t->nlinks].b = b;
+  t->nlinks++;
+}
+
+/* Slot i against slots [j0, j1): the pair predicate for every j not already
+ * in i's component.  Skipping a pair whose two particles are already
+ * connected leaves the connected components -- the partition -- unchanged. */
+static void scan_range(scan_thread *t, uint32_t i, int64_t j0, int64_t j1, double lsq) {
+  const scan_shared *sh = t->sh;
+  uint32_t *parent = t->parent;
+  uint32_t ri = uf_find(parent, i);
+  for (int64_t j = j0; j < j1; j++) {
+    uint32_t rj = uf_find(parent, (uint32_t)j);
+    if (rj == ri) continue;
+    int lk = sh->dbl ? cmh_oracle_linked_f64((const double *)sh->spos + 3 * i,
+                                             (const double *)sh->spos + 3 * j, lsq)
+                     : cmh_oracle_linked_f32((const float *)sh->spos + 3 * i,
+                                             (const float *)sh->spos + 3 * j, lsq);
+    t->ntests++;
+    if (lk) {
+      add_link(t, i, (uint32_t)j);
+      ri = uf_hook(parent, ri, rj);
+    }
+  }
+}
+
+/* The cell loop of FOF.c:96-161 over one row (iz, iy) of cells: each particle
+ * of a cell against the later particles of the same cell (FOF.c:114-119) and
+ * every particle of the 13 forward cells (FOF.c:122-153), so that each
+ * unordered cell pair is visited once. */
+static void scan_row(scan_thread *t, int iz, int iy) {
+  const scan_shared *sh = t->sh;
+  const int *nc = sh->nc;
+  for (int ix = 0; ix < nc[0]; ix++) {
+    const int64_t c = ((int64_t)iz * nc[1] + iy) * nc[0] + ix;
+    const int64_t a0 = sh->cstart[c], a1 = sh->cstart[c + 1];
+    if (a0 == a1) continue;
+    double lsq = sh->linksq;
+    if (sh->p->varlink)
+      lsq = cmh_oracle_cell_linksq(sh->p, sh->rmin_buff, sh->lcell, ix, iy, iz);
+    for (int64_t i = a0; i < a1; i++) {
+      scan_range(t, (uint32_t)i, i + 1, a1, lsq);
+      for (int iz2 = iz; iz2 <= iz + 1; iz2++) {
+        if (iz2 >= nc[2]) continue;
+        int iy1 = (iz2 == iz) ? iy : iy - 1;
+        for (int iy2 = iy1; iy2 <= iy + 1; iy2++) {
+          if (iy2 >= nc[1] || iy2 < 0) continue;
+          int ix1 = (iz2 == iz && iy2 == iy) ? ix : ix - 1;
+          for (int ix2 = ix1; ix2 <= ix + 1; ix2++) {
+            if (ix2 >= nc[0] || ix2 < 0) continue;
+            if (ix2 == ix && iy2 == iy && iz2 == iz) continue;
+            const int64_t c2 = ((int64_t)iz2 * nc[1] + iy2) * nc[0] + ix2;
+            scan_range(t, (uint32_t)i, sh->cstart[c2], sh->cstart[c2 + 1], lsq);
+          }
+        }
+      }
+    }
+  }
+}
+
+static void *scan_worker(void *arg) {
+  scan_thread *t = (scan_thread *)arg;
+  const scan_shared *sh = t->sh;
+  const int64_t nrows = (int64_t)sh->nc[2] * sh->nc[1];
+  while (!t->err) {
+    int64_t r = atomic_fetch_add(sh->next_row, 1);
+    if (r >= nrows) break;
+    scan_row(t, (int)(r / sh->nc[1]), (int)(r % sh->nc[1]));
+  }
+  return NULL;
+}
+
+/* Threads of the cell scan: CMH_ORACLE_THREADS, else the online cores; one
+ * for small inputs. */
+static int scan_threads(int64_t n_proc) {
+  if (n_proc < 200000) return 1;
+  const char *e = getenv("CMH_ORACLE_THREADS");
+  long t = e ? strtol(e, NULL, 10) : sysconf(_SC_NPROCESSORS_ONLN);
+  if (t < 1) t = 1;
+  if (t > 64) t = 64;
+  return (int)t;
 }
 
 int cmh_oracle_fof(const cmh_oracle_params *p, int64_t n_proc,
@@ -180,10 +295,15 @@ int cmh_oracle_fof(const cmh_oracle_params *p, int64_t n_proc,
                    int64_t *member, cmh_oracle_stats *st) {
   if (!p || n_proc < 0 || !group || !halo_head || !halo_props) return -1;
   if (n_proc > 0 && (!proc_pos || !proc_vel)) return -1;
+  if (n_proc >= (int64_t)0xffffffffll) return -1;
   const int dbl = p->pos_is_double;
   const int vdbl = p->vel_is_double;
-  double rmin_buff[3], rmax_buff[3], lcell[3];
-  int nc[3];
+  scan_shared sh;
+  memset(&sh, 0, sizeof sh);
+  sh.p = p;
+  sh.dbl = dbl;
+  double *rmin_buff = sh.rmin_buff, rmax_buff[3], *lcell = sh.lcell;
+  int *nc = sh.nc;
   for (int a = 0; a < 3; a++) {
     rmin_buff[a] = p->lo[a] - p->boundary;               /* startup.c:40-47 */
     rmax_buff[a] = p->hi[a] + p->boundary;
@@ -191,7 +311,7 @@ int cmh_oracle_fof(const cmh_oracle_params *p, int64_t n_proc,
     lcell[a] = (p->hi[a] - p->lo[a] + 2.0 * p->boundary) / p->cells[a]; /* FOF.c:50-52 */
     nc[a] = (int)ceil((rmax_buff[a] - rmin_buff[a]) / lcell[a]) + 1;    /* FOF.c:63-65 */
   }
-  double linksq = p->linklength * p->linklength;                        /* FOF.c:60 */
+  sh.linksq = p->linklength * p->linklength;                            /* FOF.c:60 */
   double maxlink = p->linklength;
   if (p->varlink) {
     if (p->ltab_n < 2 || !p->ltab) return -1;
@@ -202,97 +322,134 @@ int cmh_oracle_fof(const cmh_oracle_params *p, int64_t n_proc,
   for (int a = 0; a < 3; a++)
     if (maxlink > lcell[a]) return -2;
 
+  /* Cell of every particle (FOF.c:76-92).  The reference chains each cell's
+   * particles into a linked list; here they are counting-sorted into slots,
+   * each cell's particles contiguous and in ascending index order.  The
+   * order in which pairs are tested does not change the components. */
   const int64_t ncell = (int64_t)nc[0] * nc[1] * nc[2];
-  int64_t *first = (int64_t *)malloc(sizeof(int64_t) * (size_t)(ncell > 0 ? ncell : 1));
-  int64_t *chain = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_proc + 1));
-  int64_t *parent = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_proc + 1));
-  if (!first || !chain || !parent) { free(first); free(chain); free(parent); return -1; }
-  for (int64_t c = 0; c < ncell; c++) first[c] = -1;
-
-  /* set chain (FOF.c:76-92): head-of-list per cell, LIFO */
+  const size_t pw = dbl ? sizeof(double) : sizeof(float);
+  int64_t *cell = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_proc > 0 ? n_proc : 1));
+  int64_t *cstart = (int64_t *)calloc((size_t)ncell + 2, sizeof(int64_t));
+  uint32_t *slot_src = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n_proc > 0 ? n_proc : 1));
+  void *spos = malloc(3 * pw * (size_t)(n_proc > 0 ? n_proc : 1));
+  if (!cell || !cstart || !slot_src || !spos) {
+    free(cell); free(cstart); free(slot_src); free(spos);
+    return -1;
+  }
   for (int64_t i = 0; i < n_proc; i++) {
-    parent[i] = i;
     int ic[3];
     for (int a = 0; a < 3; a++) {
       double x = getpos(proc_pos, dbl, i, a);
-      if (x < rmin_buff[a] || x > rmax_buff[a]) {
-        free(first); free(chain); free(parent);
+      if (!(x >= rmin_buff[a] && x <= rmax_buff[a])) {
+        free(cell); free(cstart); free(slot_src); free(spos);
         return -3;
       }
       ic[a] = (int)floor((x - rmin_buff[a]) / lcell[a]);
     }
-    int64_t ind = ((int64_t)ic[2] * nc[1] + ic[1]) * nc[0] + ic[0];
-    chain[i] = first[ind];
-    first[ind] = i;
+    cell[i] = ((int64_t)ic[2] * nc[1] + ic[1]) * nc[0] + ic[0];
+    cstart[cell[i] + 1]++;
   }
+  for (int64_t c = 0; c < ncell; c++) cstart[c + 1] += cstart[c];
+  {
+    /* cstart[c] walks from the start to the end of cell c, then the starts
+     * are shifted back */
+    for (int64_t i = 0; i < n_proc; i++) {
+      const int64_t k = cstart[cell[i]]++;
+      slot_src[k] = (uint32_t)i;
+      memcpy((char *)spos + 3 * pw * (size_t)k, (const char *)proc_pos + 3 * pw * (size_t)i, 3 * pw);
+    }
+    for (int64_t c = ncell; c > 0; c--) cstart[c] = cstart[c - 1];
+    cstart[0] = 0;
+  }
+  free(cell);
+  sh.cstart = cstart;
+  sh.spos = spos;
 
-  int64_t ntests = 0;
-  for (int iz = 0; iz < nc[2]; iz++)
-    for (int iy = 0; iy < nc[1]; iy++)
-      for (int ix = 0; ix < nc[0]; ix++) {
-        int64_t ip = first[((int64_t)iz * nc[1] + iy) * nc[0] + ix];
-        if (ip < 0) continue;
-        double lsq = linksq;
-        if (p->varlink) lsq = cmh_oracle_cell_linksq(p, rmin_buff, lcell, ix, iy, iz);
-        do {
-          /* same cell (FOF.c:114-119) */
-          for (int64_t ip2 = chain[ip]; ip2 >= 0; ip2 = chain[ip2]) {
-            int lk = dbl ? cmh_oracle_linked_f64((const double *)proc_pos + 3 * ip,
-                                                 (const double *)proc_pos + 3 * ip2, lsq)
-                         : cmh_oracle_linked_f32((const float *)proc_pos + 3 * ip,
-                                                 (const float *)proc_pos + 3 * ip2, lsq);
-            ntests++;
-            if (lk) uf_union(parent, ip, ip2);
-          }
-          /* 13 forward cells (FOF.c:122-153) */
-          for (int iz2 = iz; iz2 <= iz + 1; iz2++) {
-            if (iz2 >= nc[2]) continue;
-            int iy1 = (iz2 == iz) ? iy : iy - 1;
-            for (int iy2 = iy1; iy2 <= iy + 1; iy2++) {
-              if (iy2 >= nc[1] || iy2 < 0) continue;
-              int ix1 = (iz2 == iz && iy2 == iy) ? ix : ix - 1;
-              for (int ix2 = ix1; ix2 <= ix + 1; ix2++) {
-                if (ix2 >= nc[0] || ix2 < 0) continue;
-                if (ix2 == ix && iy2 == iy && iz2 == iz) continue;
-                int64_t ip2 = first[((int64_t)iz2 * nc[1] + iy2) * nc[0] + ix2];
-                for (; ip2 >= 0; ip2 = chain[ip2]) {
-                  int lk = dbl ? cmh_oracle_linked_f64((const double *)proc_pos + 3 * ip,
-                                                       (const double *)proc_pos + 3 * ip2, lsq)
-                               : cmh_oracle_linked_f32((const float *)proc_pos + 3 * ip,
-                                                       (const float *)proc_pos + 3 * ip2, lsq);
-                  ntests++;
-                  if (lk) uf_union(parent, ip, ip2);
-                }
-              }
-            }
-          }
-          ip = chain[ip];
-        } while (ip >= 0);
+  /* The scan, rows of cells spread over threads.  Each thread keeps its own
+   * union-find and records the joins it makes (a spanning forest of the
+   * links it found); the forests of all threads span the same components as
+   * all links together, and are merged below. */
+  const int nt = scan_threads(n_proc);
+  _Atomic int64_t next_row = 0;
+  sh.next_row = &next_row;
+  scan_thread *th = (scan_thread *)calloc((size_t)nt, sizeof(scan_thread));
+  uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n_proc > 0 ? n_proc : 1));
+  int err = !th || !parent;
+  for (int k = 0; k < nt && !err; k++) {
+    th[k].sh = &sh;
+    th[k].parent = k == 0 ? parent : (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n_proc > 0 ? n_proc : 1));
+    if (!th[k].parent) { err = 1; break; }
+    for (int64_t i = 0; i < n_proc; i++) th[k].parent[i] = (uint32_t)i;
+  }
+  if (!err) {
+    if (nt == 1) {
+      scan_worker(&th[0]);
+    } else {
+      pthread_t *tid = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nt);
+      int started = 0;
+      if (!tid) err = 1;
+      for (int k = 0; k < nt && !err; k++) {
+        if (pthread_create(&tid[k], NULL, scan_worker, &th[k]) != 0) { err = 1; break; }
+        started++;
       }
-  free(first);
-
-  /* Retrieval.  The union-find root is the lowest index of the group, the
-   * same particle the reference's head scan (FOF.c:189-201) calls the head. */
-  int64_t *count = chain; /* reuse: count per root */
-  for (int64_t i = 0; i < n_proc; i++) count[i] = 0;
-  int64_t ngroups = 0;
-  for (int64_t i = 0; i < n_proc; i++) {
-    int64_t r = uf_find(parent, i);
-    group[i] = r;
-    if (count[r]++ == 0) ngroups++;
+      for (int k = 0; k < started; k++) pthread_join(tid[k], NULL);
+      free(tid);
+    }
   }
+  int64_t ntests = 0;
+  if (!err) {
+    /* thread 0's union-find already holds its own joins; add the others' */
+    for (int k = 1; k < nt; k++)
+      for (int64_t q = 0; q < th[k].nlinks; q++) {
+        uint32_t ra = uf_find(parent, th[k].links[q].a), rb = uf_find(parent, th[k].links[q].b);
+        if (ra != rb) uf_hook(parent, ra, rb);
+      }
+    for (int k = 0; k < nt; k++) {
+      ntests += th[k].ntests;
+      err |= th[k].err;
+    }
+  }
+  for (int k = 0; th && k < nt; k++) {
+    if (k > 0) free(th[k].parent);
+    free(th[k].links);
+  }
+  free(th);
+  free(cstart);
+  free(spos);
+  if (err) { free(parent); free(slot_src); return -1; }
+
+  /* Retrieval.  The reference's head (FOF.c:189-201) is the lowest index of
+   * the group: per component the lowest particle index of its slots. */
+  int64_t *count = (int64_t *)calloc((size_t)(n_proc > 0 ? n_proc : 1), sizeof(int64_t));
+  uint32_t *low = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n_proc > 0 ? n_proc : 1));
+  if (!count || !low) { free(count); free(low); free(parent); free(slot_src); return -1; }
+  for (int64_t k = 0; k < n_proc; k++) low[k] = 0xffffffffu;
+  for (int64_t k = 0; k < n_proc; k++) {
+    const uint32_t r = uf_find(parent, (uint32_t)k);
+    if (slot_src[k] < low[r]) low[r] = slot_src[k];
+  }
+  int64_t ngroups = 0;
+  for (int64_t k = 0; k < n_proc; k++) {
+    const int64_t h = low[uf_find(parent, (uint32_t)k)];
+    group[slot_src[k]] = h;
+    if (count[h]++ == 0) ngroups++;
+  }
+  free(low);
+  free(parent);
+  free(slot_src);
   /* members of each group in ascending index order: bucket lists */
   int64_t *mstart = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_proc + 1));
   int64_t *mlist = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_proc > 0 ? n_proc : 1));
-  if (!mstart || !mlist) { free(mstart); free(mlist); free(chain); free(parent); return -1; }
+  int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_proc > 0 ? n_proc : 1));
+  if (!mstart || !mlist || !fill) { free(mstart); free(mlist); free(fill); free(count); return -1; }
   {
     int64_t acc = 0;
     for (int64_t i = 0; i < n_proc; i++) { mstart[i] = acc; acc += count[i]; }
     mstart[n_proc] = acc;
-    int64_t *fill = parent; /* parent no longer needed after group[] */
     for (int64_t i = 0; i < n_proc; i++) fill[i] = mstart[i];
     for (int64_t i = 0; i < n_proc; i++) mlist[fill[group[i]]++] = i;
   }
+  free(fill);
   if (member)
     for (int64_t s = 0; s < n_src; s++) member[s] = -1;
 
@@ -387,7 +544,6 @@ int cmh_oracle_fof(const cmh_oracle_params *p, int64_t n_proc,
   }
   free(mstart);
   free(mlist);
-  free(chain);
-  free(parent);
+  free(count);
   return 0;
 }

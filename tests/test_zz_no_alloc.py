@@ -127,10 +127,13 @@ def test_noalloc_shell_particles_and_domain_error():
     import torch
     w = synth.config2(seed=13, scale=3000 / 256 ** 3)
     b = 6.0
+    top = np.float32(w.hi[0] + b)
+    if float(top) > w.hi[0] + b:       # the largest float32 not beyond hi + b
+        top = np.nextafter(top, np.float32(0))
     pos = w.pos.astype(np.float64)
     pos[::5] -= 0.5 * b        # into the low shell where x < b/2
-    pos = np.clip(pos, w.lo[0] - b, w.hi[0] + b).astype(np.float32)
-    pos[1] = np.float32(w.hi[0] + b)   # exactly on the outer face: inside
+    pos = np.clip(pos, w.lo[0] - b, float(top)).astype(np.float32)
+    pos[1] = top               # on the outer face: inside
     cfg = FofConfig(lo=w.lo, hi=w.hi, boundary=b, linklength=w.linklength, nphalomin=1,
                     periodic=False, precision="fp64")
     label = _labels_noalloc(pos, cfg)

@@ -641,20 +641,35 @@ struct BfStats {
   }
 };
 
-// Whether any particle of fine cell a (particles [sa, ea)) is linked to any
-// particle of fine cell b (fine coordinates bx, by, bz).  Particles of a
-// farther than the linking length from b's box are skipped.  Every 16
-// particles of a, `apart()` is asked whether a and b are still in different
+// Whether any particle of fine cell a (particles [sa, ea), fine coordinates
+// ax, ay, az) is linked to any particle of fine cell b (fine coordinates bx,
+// by, bz).  The loop runs over the cell with fewer particles, and each of
+// its particles farther than the linking length from the other cell's box
+// is skipped; the pair predicate is symmetric (the difference of a pair
+// only changes sign, and a variable length comes from the lower of the two
+// grid cells), so the orientation does not change the answer.  Every 16
+// particles, `apart()` is asked whether a and b are still in different
 // components (another thread may have joined them meanwhile); if not, the
 // search stops and reports no link, which is then harmless.
 template <class PT, bool FP32, bool VL, class Apart>
-__device__ __forceinline__ bool cells_linked(const Geom &g, uint32_t b, int bx, int by, int bz,
-                                             uint32_t sa, uint32_t ea,
+__device__ __forceinline__ bool cells_linked(const Geom &g, int ax, int ay, int az, uint32_t sa,
+                                             uint32_t ea, uint32_t b, int bx, int by, int bz,
                                              const uint32_t *__restrict__ run_start,
                                              const SPos<PT> *__restrict__ spos,
                                              const VLRec<FP32> *__restrict__ svl, BfStats &st,
                                              Apart apart) {
-  const uint32_t sb = __ldg(run_start + b), eb = __ldg(run_start + b + 1);
+  uint32_t sb = __ldg(run_start + b), eb = __ldg(run_start + b + 1);
+  if (eb - sb < ea - sa) {
+    uint32_t t = sa;
+    sa = sb;
+    sb = t;
+    t = ea;
+    ea = eb;
+    eb = t;
+    bx = ax;
+    by = ay;
+    bz = az;
+  }
   for (uint32_t i = sa; i < ea; i++) {
     if (((i - sa) & 15) == 15 && !apart()) return false;
     const SPos<PT> p = spos[i];
@@ -677,7 +692,8 @@ __device__ __forceinline__ bool cells_linked(const Geom &g, uint32_t b, int bx, 
 // since), but it stays in a's component, so "b reaches ra" still proves that
 // a and b are already joined.
 template <class PT, bool FP32, bool VL>
-__device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra, uint32_t b,
+__device__ __forceinline__ void try_link(const Geom &g, uint32_t a, int ax, int ay, int az,
+                                         uint32_t &ra, uint32_t b,
                                          int bx, int by, int bz, uint32_t sa, uint32_t ea,
                                          const uint32_t *__restrict__ run_start,
                                          const SPos<PT> *__restrict__ spos,
@@ -694,7 +710,8 @@ __device__ __forceinline__ void try_link(const Geom &g, uint32_t a, uint32_t &ra
   auto apart = [&]() {
     return uf_find_n(parent, a, st.steps) != uf_find_n(parent, b, st.steps);
   };
-  if (cells_linked<PT, FP32, VL>(g, b, bx, by, bz, sa, ea, run_start, spos, svl, st, apart)) {
+  if (cells_linked<PT, FP32, VL>(g, ax, ay, az, sa, ea, b, bx, by, bz, run_start, spos, svl, st,
+                                 apart)) {
     uf_union(parent, ra, rb, ctr);
     st.unions++;
     ra = uf_find_n(parent, ra, st.steps);
@@ -834,8 +851,8 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
               continue;
             }
             auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
-            if (cells_linked<PT, FP32, VL>(g, f + lj, gx + (tx - sx), gy + dy, gz + dz, sa, ea,
-                                           run_start, spos, svl, st, apart)) {
+            if (cells_linked<PT, FP32, VL>(g, gx, gy, gz, sa, ea, f + lj, gx + (tx - sx), gy + dy,
+                                           gz + dz, run_start, spos, svl, st, apart)) {
               if (lunion(lpar, ri, rj, ctr)) atomicSub(const_cast<uint32_t *>(ncomp), 1u);
               st.unions++;
             }
@@ -1011,7 +1028,7 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
         sa = run_start[a];
         ea = run_start[a + 1];
       }
-      try_link<PT, FP32, VL>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent,
+      try_link<PT, FP32, VL>(g, a, gx, gy, gz, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent,
                              ctr, st);
     }
     }
@@ -1146,7 +1163,7 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
       }
       const int cheb = max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz)));
       if ((PHASE == 0 && cheb > 1) || (PHASE == 1 && cheb <= 1)) continue;
-      try_link<PT, FP32, VL>(g, a, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent, ctr,
+      try_link<PT, FP32, VL>(g, a, gx, gy, gz, ra, r, bx2, by2, bz2, sa, ea, run_start, spos, svl, parent, ctr,
                              st);
     }
   }
@@ -1610,6 +1627,9 @@ Geom Plan::make_geometry(const cmh_fof_params &p, const std::vector<double> &lta
     const double sep = std::cbrt(vol / std::max<double>((double)n_in, 1.0));
     k = (int)std::lround(sep / g.h * cell_scale);
   }
+  if (g.W > kMaxCellFactor)
+    fail(CMH_ERR_INVALID_ARGUMENT, "linking lengths span too wide a range (longest / shortest "
+                                   "above 18): a fine cell's reach would leave the 27 top cells");
   k = std::min(std::max(k, g.W), kMaxCellFactor);
   while (true) {
     uint64_t T = 1;

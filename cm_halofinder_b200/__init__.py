@@ -257,21 +257,34 @@ class Plan:
                         dense_min=int(tuning["dense_min"]))
         _abi.check(self._L.cmh_plan_set_tuning(self._h, C.byref(t)))
 
-    def run_batch(self, configs, positions, velocities, stream=None):
+    def run_batch(self, configs, positions, velocities, stream=None, with_status=False):
         """Many independent boxes in one run (one sort, one befriending pass,
         one reduction for all of them); positions/velocities are torch CUDA
-        tensors.  Returns one host Catalog per box."""
+        tensors.  Returns one host Catalog per box.  with_status: each box is
+        checked on its own (cmh_plan_run_batch_status) and (catalogs,
+        statuses) is returned, a rejected box's catalog being None."""
         nb, P, parts, _keep = self._batch_args(configs, positions, velocities)
         cats = (_abi.Catalog * nb)()
-        _abi.check(self._L.cmh_plan_run_batch(self._h, P, parts, nb, cats,
-                                              C.c_void_p(self._stream(stream))))
+        st = (C.c_int * nb)()
+        sp = C.c_void_p(self._stream(stream))
+        if with_status:
+            rc = self._L.cmh_plan_run_batch_status(self._h, P, parts, nb, cats, st, sp)
+        else:
+            rc = self._L.cmh_plan_run_batch(self._h, P, parts, nb, cats, sp)
+        _abi.check(rc)
         out = []
         for b in range(nb):
             try:
-                out.append(_host_catalog(cats[b]))
+                out.append(_host_catalog(cats[b]) if (not with_status or st[b] == 0) else None)
             finally:
                 self._L.cmh_catalog_free(C.byref(cats[b]))
-        return out
+        return (out, [int(x) for x in st]) if with_status else out
+
+    def set_limits(self, union_attempts=-1, lookback_polls=-1):
+        """Bounds of the device loops that retry or wait (cmh_plan_set_limits);
+        negative keeps the default."""
+        lim = _abi.Limits(union_attempts=int(union_attempts), lookback_polls=int(lookback_polls))
+        _abi.check(self._L.cmh_plan_set_limits(self._h, C.byref(lim)))
 
     def close(self):
         if getattr(self, "_h", None):

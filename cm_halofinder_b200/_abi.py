@@ -104,6 +104,10 @@ class RunParameters(C.Structure):
         ("InputInfoFile", C.c_char * 500)]
 
 
+class Limits(C.Structure):
+    _fields_ = [("union_attempts", C.c_int64), ("lookback_polls", C.c_int64)]
+
+
 # Every symbol include/cmh_fof.h declares, with its ctypes signature.
 SIGNATURES = {
     "cmh_abi_version": (C.c_int, []),
@@ -125,6 +129,10 @@ SIGNATURES = {
                                      C.c_int32, C.POINTER(Catalog), C.c_void_p]),
     "cmh_fof_run_batch": (C.c_int, [C.POINTER(FofParams), C.POINTER(Particles), C.c_int32,
                                     C.POINTER(Catalog), C.c_void_p]),
+    "cmh_plan_run_batch_status": (C.c_int, [C.c_void_p, C.POINTER(FofParams),
+                                            C.POINTER(Particles), C.c_int32, C.POINTER(Catalog),
+                                            C.POINTER(C.c_int), C.c_void_p]),
+    "cmh_plan_set_limits": (C.c_int, [C.c_void_p, C.POINTER(Limits)]),
     "cmh_fof_labels_noalloc": (C.c_int, [C.POINTER(FofParams), C.c_void_p, C.c_int32,
                                          C.c_int64, C.c_void_p, C.c_void_p]),
     "cmh_read_parameterfile": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(RunParameters)]),

@@ -11,6 +11,7 @@
 #include <new>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "cmh_internal.cuh"
 #include "plan.cuh"
@@ -38,6 +39,20 @@ void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
 
 void fail(cmh_status code, const std::string &msg) { throw Error{code, msg}; }
 
+bool fault_active(const char *kind) {
+  const char *v = getenv("CMH_FAULT");
+  if (!v || !*v) return false;
+  const size_t n = strlen(kind);
+  for (const char *p = v; *p;) {
+    const char *e = strchr(p, ',');
+    const size_t len = e ? (size_t)(e - p) : strlen(p);
+    if (len == n && strncmp(p, kind, n) == 0) return true;
+    if (!e) break;
+    p = e + 1;
+  }
+  return false;
+}
+
 int resident_ctas(const void *kernel, int threads, size_t smem) {
   static std::mutex mu;
   static std::map<std::tuple<const void *, int, size_t, int>, int> cache;
@@ -57,6 +72,8 @@ int resident_ctas(const void *kernel, int threads, size_t smem) {
 
 void DevBuf::ensure(size_t bytes) {
   if (bytes <= cap && p) return;
+  if (fault_active("alloc"))
+    fail(CMH_ERR_OUT_OF_MEMORY, "device allocation failed (injected: CMH_FAULT=alloc)");
   if (p) CMH_CUDA(cudaFree(p));
   p = nullptr;
   cap = 0;
@@ -108,6 +125,7 @@ void Plan::release_workspace() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   graph_exec = nullptr;
   graph_sig.clear();
+  uploaded_sig.clear();
   each_buf([](DevBuf &b) { b.release(); });
   np_cap = nd_cap = nc_cap = 0;
 }
@@ -545,6 +563,81 @@ cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,
   for (int b = 0; b < nbox; b++) memset(&cats[b], 0, sizeof cats[b]);
   run_batch_on(*static_cast<Plan *>(plan), params, parts, nbox, cats,
                static_cast<cudaStream_t>(stream));
+  CMH_API_END
+}
+
+cmh_status cmh_plan_run_batch_status(cmh_plan *plan, const cmh_fof_params *params,
+                                     const cmh_particles *parts, int32_t nbox,
+                                     cmh_catalog *cats, cmh_status *box_status, void *stream) {
+  CMH_API_BEGIN
+  if (!plan || !params || !parts || !cats || !box_status || nbox < 1)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT,
+              "plan, params, particles, catalogs and statuses are required");
+  Plan &pl = *static_cast<Plan *>(plan);
+  // each box on its own: its particle description, then its geometry
+  std::vector<int> ok;
+  int precision = -1;
+  for (int b = 0; b < nbox; b++) {
+    memset(&cats[b], 0, sizeof cats[b]);
+    box_status[b] = CMH_OK;
+    try {
+      check_parts(&parts[b]);
+      if (parts[b].location != CMH_DEVICE)
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "batched runs take device-resident particles");
+      if (parts[b].pos_dtype != pl.pos_dtype)
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "position dtype differs from the plan's");
+      const cmh_fof_params &p = params[b];
+      if (!(p.linklength > 0) || !(p.boundary >= 0) ||
+          (p.precision != CMH_PLAIN_FP64 && p.precision != CMH_FP32_RECHECK))
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "bad Linklength, Boundarysize or precision");
+      if (precision >= 0 && p.precision != precision)
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "all boxes of a batch share the precision mode");
+      std::vector<double> ltab;
+      if (p.varlink) {
+        if (p.ltab_n < 2 || !p.ltab)
+          cmh::fail(CMH_ERR_INVALID_ARGUMENT, "variable linking length needs a table");
+        ltab.assign(p.ltab, p.ltab + p.ltab_n);
+      }
+      (void)pl.make_geometry(p, ltab, parts[b].n, 0);
+      precision = p.precision;
+      ok.push_back(b);
+    } catch (const Error &e) {
+      box_status[b] = e.code;
+    }
+  }
+  if (ok.empty()) return CMH_OK;
+  std::vector<cmh_fof_params> sp;
+  std::vector<cmh_particles> sq;
+  std::vector<cmh_catalog> sc(ok.size());
+  for (int b : ok) {
+    sp.push_back(params[b]);
+    sq.push_back(parts[b]);
+  }
+  try {
+    run_batch_on(pl, sp.data(), sq.data(), (int32_t)ok.size(), sc.data(),
+                 static_cast<cudaStream_t>(stream));
+  } catch (const Error &e) {
+    for (cmh_catalog &c : sc) cmh_catalog_free(&c);
+    for (int b : ok) box_status[b] = e.code;
+    throw;
+  }
+  for (size_t i = 0; i < ok.size(); i++) cats[ok[i]] = sc[i];
+  CMH_API_END
+}
+
+cmh_status cmh_plan_set_limits(cmh_plan *plan, const cmh_limits *limits) {
+  CMH_API_BEGIN
+  if (!plan || !limits) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and limits are required");
+  auto pick = [](int64_t v, uint32_t def) -> uint32_t {
+    if (v < 0) return def;
+    if (v > 0x7fffffffll) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "limits must be below 2^31");
+    return (uint32_t)v;
+  };
+  const uint32_t u = pick(limits->union_attempts, cmh::kUnionCap);
+  const uint32_t w = pick(limits->lookback_polls, cmh::kSpinCap);
+  Plan &pl = *static_cast<Plan *>(plan);
+  pl.union_cap = u;
+  pl.spin_cap = w;
   CMH_API_END
 }
 

@@ -33,6 +33,13 @@ extern thread_local long long g_launches;
   } while (0)
 [[noreturn]] void fail(cmh_status code, const std::string &msg);
 
+// Host-side fault injection for tests: whether `kind` is one of the
+// comma-separated words of the CMH_FAULT environment variable (alloc: device
+// allocations fail; io: opening a file fails; overflow: every run overflows
+// its capacity; lookback: one tile of the cell sort publishes nothing, so a
+// capped device wait runs out).  Read on every call, in host code only.
+bool fault_active(const char *kind);
+
 // Grid size for a grid-stride kernel: a multiple of the SM count, capped by
 // the work.
 inline unsigned grid_for(int64_t n, int threads, int per_sm = 8) {
@@ -74,6 +81,17 @@ void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n,
                         const uint32_t *n_dev = nullptr);
 
 // ---- radix_sort.cu -----------------------------------------------------------
+// Bounds of the sorts' look-back waits: a tile polls a lower tile's state at
+// most spin_cap times, then gives up (the sort's giveups counter is raised;
+// its output is then not an ordering).  stall_tile (a test hook) names a tile
+// of the first pass that publishes nothing, so that its successor's wait
+// runs out.
+constexpr uint32_t kSpinCap = 1u << 22;
+struct SortWaits {
+  uint32_t spin_cap = kSpinCap;
+  uint32_t stall_tile = 0xffffffffu;
+};
+
 // Stable LSD radix sort of (key u64, value u32) pairs on the low `bits` key
 // bits.  Result lands in keys/vals (the alt buffers are scratch); `tmp`
 // holds the digit counts and the tiles' look-back states.
@@ -86,7 +104,7 @@ void exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n,
 void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s,
-                        bool copy_back = true);
+                        bool copy_back = true, SortWaits waits = SortWaits{});
 // The values of the same sort, in key order, without the sorted keys: both
 // key buffers end as scratch (the later passes move 32-bit key words, with
 // 9-bit digits where that saves a pass), and the values end in vals_alt
@@ -94,11 +112,13 @@ void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
 int radix_order_passes(int bits);
 void radix_order_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                          uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s);
+                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s,
+                         SortWaits waits = SortWaits{});
 // Same for 32-bit keys.
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s);
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s,
+                        SortWaits waits = SortWaits{});
 // Scratch bytes of a sort of up to n keys.
 size_t radix_sort_scratch(int64_t n);
 

@@ -362,6 +362,7 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
                                                      uint64_t *__restrict__ cells,
                                                      uint32_t *__restrict__ flag,
                                                      const DevScal *__restrict__ sc) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   __shared__ uint64_t s_base[kMaxBoxes];
   load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
@@ -411,6 +412,7 @@ __global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ cells,
                                              uint32_t *__restrict__ run_start,
                                              uint64_t *__restrict__ run_g,
                                              uint16_t *__restrict__ run_box) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   __shared__ uint64_t s_base[kMaxBoxes];
   load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
@@ -438,6 +440,7 @@ __global__ void __launch_bounds__(kT) k_varlink_recs(const SPos<PT> *__restrict_
                                                      const BoxDev *__restrict__ boxes,
                                                      const DevScal *__restrict__ sc,
                                                      VLRec<FP32> *__restrict__ svl) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const int64_t np = sc->np;
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const Geom &g = boxes[run_box[run_of[i]]].g;
@@ -475,6 +478,7 @@ __global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ 
                                                    const BoxDev *__restrict__ boxes,
                                                    const DevScal *__restrict__ sc,
                                                    uint32_t *__restrict__ top_range) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
     const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
@@ -493,6 +497,7 @@ __global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__
                                                     const uint2 *__restrict__ top_range,
                                                     uint32_t dense_min,
                                                     uint32_t *__restrict__ flag) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < (int64_t)R; r += gstride()) {
     const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
@@ -520,6 +525,7 @@ __global__ void __launch_bounds__(kT) k_dense_slots(const uint64_t *__restrict__
                                                     uint32_t *__restrict__ top_slot,
                                                     uint2 *__restrict__ dense_range,
                                                     uint32_t *__restrict__ big) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
     if (!dflag[r]) continue;
@@ -534,11 +540,13 @@ __global__ void __launch_bounds__(kT) k_dense_slots(const uint64_t *__restrict__
 }
 
 __global__ void k_clamp_dense(DevScal *sc, uint32_t nd_cap) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   if (threadIdx.x == 0 && blockIdx.x == 0 && sc->nd > nd_cap) atomicOr(&sc->overflow, 2u);
 }
 
 __global__ void __launch_bounds__(kT) k_iota(uint32_t *__restrict__ a,
                                              const DevScal *__restrict__ sc) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) a[r] = (uint32_t)r;
 }
@@ -712,7 +720,7 @@ __device__ __forceinline__ void try_link(const Geom &g, uint32_t a, int ax, int 
   };
   if (cells_linked<PT, FP32, VL>(g, ax, ay, az, sa, ea, b, bx, by, bz, run_start, spos, svl, st,
                                  apart)) {
-    uf_union(parent, ra, rb, ctr);
+    uf_union(parent, ra, rb, ctr, g.union_cap);
     st.unions++;
     ra = uf_find_n(parent, ra, st.steps);
   }
@@ -732,8 +740,9 @@ __device__ __forceinline__ uint32_t lfind(volatile uint32_t *lp, uint32_t x) {
 }
 
 // Returns whether this call joined two components.
-__device__ __forceinline__ bool lunion(uint32_t *lp, uint32_t a, uint32_t b, Counters *ctr) {
-  for (int it = 0; it < kUnionCap; it++) {
+__device__ __forceinline__ bool lunion(uint32_t *lp, uint32_t a, uint32_t b, Counters *ctr,
+                                       uint32_t cap) {
+  for (uint32_t it = 0; it < cap; it++) {
     a = lfind(lp, a);
     b = lfind(lp, b);
     if (a == b) return false;
@@ -853,7 +862,8 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
             auto apart = [&]() { return lfind(lpar, i) != lfind(lpar, lj); };
             if (cells_linked<PT, FP32, VL>(g, gx, gy, gz, sa, ea, f + lj, gx + (tx - sx), gy + dy,
                                            gz + dz, run_start, spos, svl, st, apart)) {
-              if (lunion(lpar, ri, rj, ctr)) atomicSub(const_cast<uint32_t *>(ncomp), 1u);
+              if (lunion(lpar, ri, rj, ctr, g.union_cap))
+                atomicSub(const_cast<uint32_t *>(ncomp), 1u);
               st.unions++;
             }
           }
@@ -886,6 +896,7 @@ __global__ void __launch_bounds__(128) k_befriend_dense(
     uint32_t nd_cap, uint32_t *__restrict__ grows, uint32_t kk,
     const SPos<PT> *__restrict__ spos, const VLRec<FP32> *__restrict__ svl, uint32_t *parent,
     Counters *ctr, uint32_t lstride) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   extern __shared__ uint32_t smem[];
   __shared__ uint32_t s_slot;
   const uint32_t nd = min(sc->nd, nd_cap), nbig = sc->nbig;
@@ -946,6 +957,7 @@ __global__ void __launch_bounds__(kT, 5) k_befriend_simple(
     const uint32_t *__restrict__ top_slot, const SPos<PT> *__restrict__ spos,
     const VLRec<FP32> *__restrict__ svl, uint32_t *parent, uint32_t *__restrict__ queue,
     Counters *ctr) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   const int lane = threadIdx.x & 31;
   __shared__ uint32_t s_base;
@@ -1053,6 +1065,7 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
     const uint32_t *__restrict__ top_slot,
     const uint32_t *__restrict__ grows, uint32_t kk, const SPos<PT> *__restrict__ spos,
     const VLRec<FP32> *__restrict__ svl, uint32_t *parent, Counters *ctr) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t NQ = sc->qcount;
   uint32_t *next = PHASE == 0 ? &sc->next0 : &sc->next1;
   const int lane = threadIdx.x & 31;
@@ -1172,6 +1185,7 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
 
 __global__ void __launch_bounds__(kT) k_compress(uint32_t *parent,
                                                  const DevScal *__restrict__ sc) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) parent[r] = uf_find(parent, (uint32_t)r);
 }
@@ -1229,6 +1243,7 @@ __global__ void __launch_bounds__(kT) k_group_count(const uint32_t *__restrict__
                                                     const DevScal *__restrict__ sc,
                                                     uint32_t *__restrict__ count,
                                                     uint32_t *__restrict__ head) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const int64_t np = sc->np;
   const int64_t n_iter = (np + 31) / 32 * 32;
   for (int64_t i = gtid(); i < n_iter; i += gstride()) {
@@ -1268,6 +1283,7 @@ __global__ void __launch_bounds__(kT) k_subsample(
     const BoxDev *__restrict__ boxes, const uint32_t *__restrict__ boxd, int nbox,
     const DevScal *__restrict__ sc, const uint64_t *__restrict__ ids, double samp_in,
     double samp_out, uint64_t seed, int closed, uint8_t *__restrict__ samp) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const int64_t np = sc->np;
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const uint32_t run = run_of[i];
@@ -1298,6 +1314,7 @@ __global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ 
                                                    const DevScal *__restrict__ sc,
                                                    uint32_t *__restrict__ flag,
                                                    unsigned long long *ngroups) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   unsigned long long roots = 0;
   // (the scan of the flags reads the first R only)
@@ -1316,6 +1333,7 @@ __global__ void __launch_bounds__(kT) k_cand_list(const uint32_t *__restrict__ f
                                                   const DevScal *__restrict__ sc,
                                                   uint32_t *__restrict__ cand_of_root,
                                                   uint32_t *__restrict__ cand_root) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
   for (int64_t r = gtid(); r < R; r += gstride()) {
     if (!flag[r]) continue;
@@ -1334,6 +1352,7 @@ __global__ void __launch_bounds__(kT) k_group_sums(
     const BoxDev *__restrict__ boxes, const SPos<PT> *__restrict__ spos,
     const DevScal *__restrict__ sc, int props, double *__restrict__ sums,
     uint32_t *__restrict__ warn) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const int64_t np = sc->np;
   const int64_t n_iter = (np + 31) / 32 * 32;
   for (int64_t i = gtid(); i < n_iter; i += gstride()) {
@@ -1400,6 +1419,7 @@ __global__ void __launch_bounds__(kT) k_owned(const double *__restrict__ sums,
                                               const BoxDev *__restrict__ boxes,
                                               const DevScal *__restrict__ sc, int64_t cap,
                                               uint32_t *__restrict__ own) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t nc = sc->nc;
   for (int64_t c = gtid(); c < cap; c += gstride()) {
     bool ok = false;
@@ -1425,6 +1445,7 @@ __global__ void __launch_bounds__(kT) k_own_list(const uint32_t *__restrict__ ow
                                                  const DevScal *__restrict__ sc,
                                                  uint32_t *__restrict__ okeys,
                                                  uint32_t *__restrict__ ovals) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t nc = sc->nc;
   for (int64_t c = gtid(); c < nc; c += gstride()) {
     if (!own[c]) continue;
@@ -1450,6 +1471,7 @@ __global__ void __launch_bounds__(kT) k_catalog(const uint32_t *__restrict__ oke
                                                 uint32_t *__restrict__ head_out,
                                                 uint32_t *__restrict__ cat_of_cand,
                                                 unsigned long long *n_warn) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t nh = sc->nh;
   for (int64_t h = gtid(); h < nh; h += gstride()) {
     const uint32_t c = ovals[h];
@@ -1513,6 +1535,7 @@ __global__ void __launch_bounds__(kT) k_member(const uint32_t *__restrict__ run_
                                                const SPos<PT> *__restrict__ spos,
                                                const DevScal *__restrict__ sc,
                                                unsigned long long *__restrict__ member) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const int64_t np = sc->np;
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const uint32_t ci = cand_of_root[parent[run_of[i]]];
@@ -1531,6 +1554,7 @@ __global__ void __launch_bounds__(kT) k_member_copy(
     const SPos<PT> *__restrict__ spos, const uint32_t *__restrict__ perm,
     const DevScal *__restrict__ sc, const unsigned long long *__restrict__ member,
     uint32_t *__restrict__ member_proc, float *__restrict__ member_pos, Counters *ctr) {
+  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const int64_t np = sc->np;
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const uint32_t run = run_of[i];
@@ -1745,9 +1769,12 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   // ---- sort ----
   // the sort leaves the indices in cell order in b_vals and no sorted keys:
   // k_gather_flags recomputes the fine cells into b_keys from the positions
+  // a look-back that gives up raises sc->failed, and every later kernel of
+  // the run then returns at once (the order would not be valid)
   radix_order_u64_u32(emit_k, emit_v, odd ? b_keys.as<uint64_t>() : b_keys_alt.as<uint64_t>(),
                       odd ? b_vals.as<uint32_t>() : b_vals_alt.as<uint32_t>(), npc, &sc->np,
-                      key_bits, sort_tmp, &c->sort_giveups, s);
+                      key_bits, sort_tmp, &sc->failed, s,
+                      SortWaits{spin_cap, stall_sort ? 1u : 0xffffffffu});
   mark(1);
   // ---- runs, top-cell ranges, dense top cells ----
   uint32_t *flag = b_keys_alt.as<uint32_t>();  // reuse: [flag | run_scan]
@@ -1906,7 +1933,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_LAUNCHED();
   radix_sort_u32_u32(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), b_okeys_alt.as<uint32_t>(),
                      b_ovals_alt.as<uint32_t>(), ncc, &sc->nh, bits_for((uint64_t)npc),
-                     sort_tmp, &c->sort_giveups, s);
+                     sort_tmp, &sc->failed, s, SortWaits{spin_cap, 0xffffffffu});
   CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, (size_t)ncc * 4, s));
 #define CMH_CATALOG(NSV)                                                                        \
   k_catalog<NSV><<<rg(k_catalog<NSV>, ncc), kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc,          \
@@ -1955,6 +1982,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
     BoxDev &bd = boxes_host[b];
     memset(&bd, 0, sizeof bd);
     bd.g = make_geometry(sp.params, sp.ltab, sp.n, sp.cell_factor);
+    bd.g.union_cap = union_cap;
     if (props < 0) props = bd.g.props;
     if (bd.g.props != props) fail(CMH_ERR_INVALID_ARGUMENT, "boxes of a run share the property set");
     bd.pos = sp.pos;
@@ -2090,9 +2118,13 @@ void Plan::read_back(cudaStream_t s, bool timed) {
                            cudaMemcpyDeviceToHost, s));
   CMH_CUDA(cudaStreamSynchronize(s));
   last = hs_;
+  // CMH_FAULT=overflow: the run is treated as having outgrown its buffers, so
+  // it is repeated with room until the attempts run out (CMH_ERR_CAPACITY),
+  // as a rank whose receive buffer overflows stops (read_data.c:551-556)
+  if (fault_active("overflow")) last.overflow |= 1u;
   if (hc.c.uf_giveups)
     fail(CMH_ERR_DEVICE_TIMEOUT, "union-find retry loop reached its iteration cap");
-  if (hc.c.sort_giveups)
+  if (hs_.failed)
     fail(CMH_ERR_DEVICE_TIMEOUT, "radix sort look-back wait reached its cap");
   stats = cmh_stats{};
   stats.n_in = n_total;
@@ -2140,10 +2172,12 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     memcpy(&samp_bits[0], &samp_in, 8);
     memcpy(&samp_bits[1], &samp_out, 8);
     samp_bits[2] = (int64_t)samp_seed ^ ((int64_t)samp_closed << 40);
-    const int64_t caps[10] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
+    stall_sort = fault_active("lookback");
+    const int64_t caps[12] = {np_cap, nd_cap, nc_cap, (int64_t)want_member, (int64_t)fp32,
                               (int64_t)dense_min, (int64_t)vel_wait,
                               sampling ? samp_bits[0] : -1, samp_bits[1],
-                              samp_bits[2] ^ (int64_t)(uintptr_t)samp_ids};
+                              samp_bits[2] ^ (int64_t)(uintptr_t)samp_ids,
+                              (int64_t)spin_cap, (int64_t)stall_sort};
     sig.insert(sig.end(), (const unsigned char *)caps, (const unsigned char *)caps + sizeof caps);
     // and the workspace addresses the recorded launches use
     each_buf([&](DevBuf &b) {
@@ -2152,13 +2186,18 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     sig.insert(sig.end(), (const unsigned char *)ltab_all.data(),
                (const unsigned char *)(ltab_all.data() + ltab_all.size()));
     const bool same = graph_exec && sig == graph_sig;
-    if (!same) {
+    // the device box table (and length tables) hold the last uploaded shape,
+    // which an eager run of another shape may have replaced since the graph
+    // was recorded: upload whenever they differ from this run's
+    if (sig != uploaded_sig) {
+      uploaded_sig.clear();
       CMH_CUDA(cudaMemcpyAsync(b_boxes.p, boxes_host.data(), sizeof(BoxDev) * boxes_host.size(),
                                cudaMemcpyHostToDevice, s));
       if (varlink)
         CMH_CUDA(cudaMemcpyAsync(ltab_dev.p, ltab_all.data(), ltab_all.size() * sizeof(double),
                                  cudaMemcpyHostToDevice, s));
       CMH_CUDA(cudaStreamSynchronize(s));
+      uploaded_sig = sig;
     }
     const long long l0 = g_launches;
     if (use_graph && same) {

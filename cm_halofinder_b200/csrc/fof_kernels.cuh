@@ -43,6 +43,7 @@ struct Geom {
   uint32_t kmul;         // floor(2^32 / k) + 1: x / k == umulhi(x, kmul) for x < 2^27
   int props;             // CMH_PROP_* bits
   int hs;                // floats per halo record
+  uint32_t union_cap;    // retries of a union before it gives up (the plan's limit)
   // variable linking length
   int varlink;
   double origin[3];
@@ -74,6 +75,8 @@ struct DevScal {
   uint32_t overflow;               // bit 0: processed particles above capacity
   uint32_t nbig, next_big;          // dense top cells handled by a whole CTA
   uint32_t next_simple;             // fine cells taken by the sparse path
+  uint32_t failed;                  // a sort's capped look-back wait gave up: every
+                                    // later kernel of the run returns at once
 };
 
 // Running counters of one run, in device memory.
@@ -234,11 +237,14 @@ __device__ __forceinline__ uint32_t uf_find_n(uint32_t *parent, uint32_t x,
   }
 }
 
-constexpr int kUnionCap = 1 << 22;
+constexpr uint32_t kUnionCap = 1u << 22;  // default retries of a union
 
+// Joins the components of a and b; retries after a lost race at most `cap`
+// times, then counts a give-up (the run reports CMH_ERR_DEVICE_TIMEOUT;
+// parents stay valid cell indices, so nothing downstream leaves its bounds).
 __device__ __forceinline__ void uf_union(uint32_t *parent, uint32_t a, uint32_t b,
-                                         Counters *ctr) {
-  for (int it = 0; it < kUnionCap; it++) {
+                                         Counters *ctr, uint32_t cap = kUnionCap) {
+  for (uint32_t it = 0; it < cap; it++) {
     a = uf_find(parent, a);
     b = uf_find(parent, b);
     if (a == b) return;

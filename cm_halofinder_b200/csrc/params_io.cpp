@@ -13,6 +13,7 @@
 
 namespace cmh {
 void set_error(const std::string &msg);
+bool fault_active(const char *kind);  // api.cu: CMH_FAULT host-side fault injection
 }
 
 namespace {
@@ -25,6 +26,9 @@ struct Tag {
   void *addr;
   bool seen;
 };
+
+// An output file, or NULL when it cannot be opened (or CMH_FAULT=io says so).
+FILE *open_out(const char *fname) { return cmh::fault_active("io") ? nullptr : fopen(fname, "w"); }
 
 cmh_status io_fail(const std::string &msg) {
   cmh::set_error(msg);
@@ -202,7 +206,7 @@ cmh_status cmh_write_halos(const char *base, int32_t task, const cmh_catalog *ca
   }
   char fname[1100];
   snprintf(fname, sizeof fname, "%s.%d", base, task);
-  FILE *fp = fopen(fname, "w");
+  FILE *fp = open_out(fname);
   if (!fp) return io_fail(std::string("Unable to open output file ") + fname);
   bool ok = true;
   const int32_t nhi = (int32_t)nh;
@@ -276,7 +280,7 @@ cmh_status cmh_write_info_sampled(const char *base, const cmh_run_parameters *rp
   }
   char fname[1100];
   snprintf(fname, sizeof fname, "%s.info", base);
-  FILE *fp = fopen(fname, "w");
+  FILE *fp = open_out(fname);
   if (!fp) return io_fail(std::string("Can't write in file ") + fname);
   fprintf(fp, "#    FILENUM      XMIN         YMIN        ZMIN         XMAX         YMAX         ZMAX         NHALOS     NSUBSAMPIN     NSUBSAMPOUT    \n");
   const int Nx = rp->Nx, Ny = rp->Ny, Nz = rp->Nz;
@@ -327,7 +331,7 @@ cmh_status cmh_write_subsample(const char *base, int32_t task, int32_t in,
   };
   char fname[1100];
   snprintf(fname, sizeof fname, "%s_%s.%d", base, in ? "inhalo" : "outhalo", task);
-  FILE *fp = fopen(fname, "w");
+  FILE *fp = open_out(fname);
   if (!fp) return io_fail(std::string("Unable to open output file ") + fname);
   bool ok = true;
   if (unf) {

@@ -33,6 +33,10 @@ struct Plan : public cmh_plan {
   bool use_graph = true;    // replay the captured run when its shape repeats
   uint32_t dense_min = 16;  // top cells with more occupied fine cells get a map
   double cell_scale = 1.0;  // autotuned scale of the default cell-size factor
+  // bounds of the device loops that retry or wait (cmh_plan_set_limits)
+  uint32_t union_cap = kUnionCap;  // retries of one union after a lost race
+  uint32_t spin_cap = kSpinCap;    // polls of one sort tile state
+  bool stall_sort = false;         // CMH_FAULT=lookback for this run
 
   // shape of the current run
   std::vector<BoxDev> boxes_host;
@@ -55,6 +59,7 @@ struct Plan : public cmh_plan {
   cudaEvent_t stage_ev[7] = {};  // boundaries between the eight stages
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<unsigned char> graph_sig;
+  std::vector<unsigned char> uploaded_sig;  // shape whose box table is on the device
   cudaStream_t cap_stream = nullptr;  // the stream runs are recorded on
   // host-resident inputs: velocities are copied on a side stream while the
   // run's first stages go on, and the property sums wait for them

@@ -29,7 +29,6 @@ constexpr int kMaxPasses = 8;
 // in the high half, the count in the low half, written in one store.
 constexpr uint64_t kAggregate = 1ull << 32;  // count = the tile's own keys of the digit
 constexpr uint64_t kInclusive = 2ull << 32;  // count = keys of the digit up to this tile
-constexpr int kSpinCap = 1 << 22;            // polls of one state before giving up
 
 template <int BINS = kBins, class K>
 __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
@@ -151,7 +150,7 @@ __global__ void __launch_bounds__(kSThreads, (sizeof(K) == 4 && BINS == BINS) ? 
     const uint32_t *__restrict__ n_dev, int shift, int out_shift,
     const uint32_t *__restrict__ goff,
     uint64_t *__restrict__ state, uint32_t *__restrict__ tile_ctr,
-    unsigned int *__restrict__ giveups) {
+    unsigned int *__restrict__ giveups, SortWaits waits) {
   const int64_t n = n_dev ? (int64_t)*n_dev : n_cap;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem<K, BINS> &sm = *reinterpret_cast<ScatterSmem<K, BINS> *>(smem_raw);
@@ -180,7 +179,9 @@ __global__ void __launch_bounds__(kSThreads, (sizeof(K) == 4 && BINS == BINS) ? 
     if (base + (int64_t)warp * 32 * kSIPT + j * 32 + lane < n)
       atomicAdd(&sm.thist[digit_of<BINS>(k[j], shift)], 1u);
   __syncthreads();
-  if (threadIdx.x < BINS)
+  // (a tile named by waits.stall_tile publishes nothing: a test hook whose
+  // successor's capped wait then runs out)
+  if (threadIdx.x < BINS && tile != waits.stall_tile)
     atomicExch(reinterpret_cast<unsigned long long *>(state + (uint64_t)tile * BINS + threadIdx.x),
                (unsigned long long)((tile == 0 ? kInclusive : kAggregate) | sm.thist[threadIdx.x]));
 #pragma unroll
@@ -228,7 +229,8 @@ __global__ void __launch_bounds__(kSThreads, (sizeof(K) == 4 && BINS == BINS) ? 
         for (int64_t j = (int64_t)tile - 1; j >= 0; j--) {
           const uint64_t *p = state + (uint64_t)j * BINS + d;
           uint64_t w = load_state(p);
-          for (int spin = 0; (w >> 32) == 0 && spin < kSpinCap; spin++) w = load_state(p);
+          for (uint32_t spin = 0; (w >> 32) == 0 && spin < waits.spin_cap; spin++)
+            w = load_state(p);
           if ((w >> 32) == 0) {
             atomicAdd(giveups, 1u);
             break;
@@ -236,8 +238,9 @@ __global__ void __launch_bounds__(kSThreads, (sizeof(K) == 4 && BINS == BINS) ? 
           excl += (uint32_t)w;
           if ((w >> 32) == 2) break;
         }
-        atomicExch(reinterpret_cast<unsigned long long *>(mine),
-                   (unsigned long long)(kInclusive | (uint64_t)(excl + acc)));
+        if (tile != waits.stall_tile)
+          atomicExch(reinterpret_cast<unsigned long long *>(mine),
+                     (unsigned long long)(kInclusive | (uint64_t)(excl + acc)));
       }
       sm.gofs[d] = goff[d] + excl;
     }
@@ -321,7 +324,7 @@ PassDigits plan_passes(int bits, bool narrow, int *wide) {
 template <class K>
 void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, int64_t n,
                      const uint32_t *n_dev, int bits, DevBuf &tmp, unsigned int *giveups,
-                     cudaStream_t s, bool copy_back, bool narrow) {
+                     cudaStream_t s, bool copy_back, bool narrow, SortWaits waits) {
   if (bits <= 0) return;
   if (bits > (int)(8 * sizeof(K)) || (bits + 7) / 8 > kMaxPasses)
     fail(CMH_ERR_INVALID_ARGUMENT, "radix sort: key bits out of range");
@@ -362,25 +365,27 @@ void radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, i
     const int bins = 1 << pd.width[p];
     CMH_CUDA(cudaMemsetAsync(state, 0, (size_t)ntiles * bins * sizeof(uint64_t), s));
     const uint32_t *go = goff + p * kMaxBins;
+    // the stall hook applies to the first pass only
+    const SortWaits wp{waits.spin_cap, p == 0 ? waits.stall_tile : 0xffffffffu};
     if (p < m && !(narrow && p == m - 1)) {
       k_rs_scatter<K, K, kBins><<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<K, kBins>), s>>>(
           static_cast<const K *>(src_k), src_v, static_cast<K *>(dst_k), dst_v, n, n_dev,
-          pd.shift[p], 0, go, state, tile_ctr + p, giveups);
+          pd.shift[p], 0, go, state, tile_ctr + p, giveups, wp);
     } else if (p < m) {
       k_rs_scatter<K, uint32_t, kBins>
           <<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<K, kBins>), s>>>(
               static_cast<const K *>(src_k), src_v, static_cast<uint32_t *>(dst_k), dst_v, n,
-              n_dev, pd.shift[p], 8 * m, go, state, tile_ctr + p, giveups);
+              n_dev, pd.shift[p], 8 * m, go, state, tile_ctr + p, giveups, wp);
     } else if (bins == kMaxBins) {
       k_rs_scatter<uint32_t, uint32_t, kMaxBins>
           <<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<uint32_t, kMaxBins>), s>>>(
               static_cast<const uint32_t *>(src_k), src_v, static_cast<uint32_t *>(dst_k), dst_v,
-              n, n_dev, pd.shift[p] - 8 * m, 0, go, state, tile_ctr + p, giveups);
+              n, n_dev, pd.shift[p] - 8 * m, 0, go, state, tile_ctr + p, giveups, wp);
     } else {
       k_rs_scatter<uint32_t, uint32_t, kBins>
           <<<(unsigned)ntiles, kSThreads, sizeof(ScatterSmem<uint32_t, kBins>), s>>>(
               static_cast<const uint32_t *>(src_k), src_v, static_cast<uint32_t *>(dst_k), dst_v,
-              n, n_dev, pd.shift[p] - 8 * m, 0, go, state, tile_ctr + p, giveups);
+              n, n_dev, pd.shift[p] - 8 * m, 0, go, state, tile_ctr + p, giveups, wp);
     }
     CMH_LAUNCHED();
     std::swap(src_k, dst_k);
@@ -408,23 +413,24 @@ int radix_order_passes(int bits) {
 
 void radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s, bool copy_back) {
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s, bool copy_back,
+                        SortWaits waits) {
   radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
-                            copy_back, false);
+                            copy_back, false, waits);
 }
 
 void radix_order_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt,
                          uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s) {
+                         DevBuf &tmp, unsigned int *giveups, cudaStream_t s, SortWaits waits) {
   radix_sort_impl<uint64_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
-                            false, true);
+                            false, true, waits);
 }
 
 void radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt,
                         uint32_t *vals_alt, int64_t n, const uint32_t *n_dev, int bits,
-                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s) {
+                        DevBuf &tmp, unsigned int *giveups, cudaStream_t s, SortWaits waits) {
   radix_sort_impl<uint32_t>(keys, vals, keys_alt, vals_alt, n, n_dev, bits, tmp, giveups, s,
-                            true, false);
+                            true, false, waits);
 }
 
 }  // namespace cmh

@@ -13,6 +13,7 @@
 #include "../../include/cmh_fof.h"
 
 namespace cmh {
+bool fault_active(const char *kind);  // api.cu: CMH_FAULT host-side fault injection
 void set_error(const std::string &msg);
 }
 
@@ -60,7 +61,7 @@ struct File {
   FILE *fp = nullptr;
   std::string name;
   File(const std::string &n, const char *mode) : name(n) {
-    fp = fopen(n.c_str(), mode);
+    fp = cmh::fault_active("io") ? nullptr : fopen(n.c_str(), mode);
     if (!fp) fail(CMH_ERR_IO, "unable to open file " + n);
   }
   ~File() {

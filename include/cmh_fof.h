@@ -149,6 +149,17 @@ int cmh_abi_version(void);
 /* Message of the last failing call on this host thread. */
 size_t cmh_last_error(char *buf, size_t len);
 
+/* Fault injection for tests (host side only, no GPU fault): the environment
+ * variable CMH_FAULT holds comma-separated words, read on every call --
+ *   alloc    : a device allocation fails (CMH_ERR_OUT_OF_MEMORY)
+ *   io       : opening an input or output file fails (CMH_ERR_IO), as the
+ *              reference's file helpers stop the run (main.c:83-112)
+ *   overflow : every run outgrows its buffers until the plan gives up
+ *              (CMH_ERR_CAPACITY), as a rank's receive-buffer overflow stops
+ *              the reference (read_data.c:551-556)
+ *   lookback : one tile of the cell sort publishes nothing, so that the next
+ *              tile's wait runs into its bound (CMH_ERR_DEVICE_TIMEOUT)   */
+
 /* ---- one-shot run: replaces void FOF(void) (src_v2/FOF.c:23, vars.h:121) - */
 
 /* Runs FoF on one domain and fills `cat` (host arrays, freed by
@@ -209,10 +220,37 @@ cmh_status cmh_plan_autotune(cmh_plan *plan, const cmh_fof_params *params,
 cmh_status cmh_plan_set_tuning(cmh_plan *plan, const cmh_tuning *tuning);
 
 /* cmh_fof_run_batch on a plan: repeated batches of the same shape replay one
- * CUDA graph. */
+ * CUDA graph.  Any box's error fails the whole call. */
 cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,
                               const cmh_particles *parts, int32_t nbox, cmh_catalog *cats,
                               void *stream);
+
+/* cmh_plan_run_batch with a status per box, so that one bad box does not
+ * fail the others: each box's parameters and particle description are
+ * checked on their own (box_status[b] = the error, cats[b] left empty), and
+ * the boxes that pass run together as one batch.  Returns CMH_OK when that
+ * batch ran (or no box passed); if the batch itself fails, every box in it
+ * gets the batch's status, which is also returned.  The reference's FOF()
+ * stops the whole run on any error (FatalError, main.c:107-112). */
+cmh_status cmh_plan_run_batch_status(cmh_plan *plan, const cmh_fof_params *params,
+                                     const cmh_particles *parts, int32_t nbox,
+                                     cmh_catalog *cats, cmh_status *box_status, void *stream);
+
+/* Bounds of the device loops that retry or wait.  A union of two
+ * union-find components (find both roots, hook one under the other) is
+ * attempted at most union_attempts times -- it is attempted again only after
+ * losing a race to another thread -- and a tile of a radix sort polls a lower
+ * tile's state at most lookback_polls times after its first read.  A loop
+ * that runs out makes the run return CMH_ERR_DEVICE_TIMEOUT (the plan stays
+ * usable; the next run starts afresh).  Negative: the default, 2^22 each.
+ * union_attempts = 0 makes every union give up at once (a test setting).
+ * The reference has no such loops (one CPU thread per rank). */
+typedef struct cmh_limits {
+  int64_t union_attempts;
+  int64_t lookback_polls;
+} cmh_limits;
+
+cmh_status cmh_plan_set_limits(cmh_plan *plan, const cmh_limits *limits);
 
 void cmh_plan_destroy(cmh_plan *plan);
 

@@ -41,7 +41,7 @@ def test_structs_match_header_layout(tmp_path):
     import subprocess
     structs = {"cmh_fof_params": _abi.FofParams, "cmh_particles": _abi.Particles,
                "cmh_stats": _abi.Stats, "cmh_catalog": _abi.Catalog,
-               "cmh_run_parameters": _abi.RunParameters}
+               "cmh_run_parameters": _abi.RunParameters, "cmh_limits": _abi.Limits}
     prog = tmp_path / "sz.c"
     prog.write_text('#include <stdio.h>\n#include "cmh_fof.h"\nint main(void){\n' + "".join(
         f'printf("%zu\\n", sizeof({k}));\n' for k in structs) + "return 0;}\n")

@@ -113,3 +113,32 @@ def test_host_inputs_repeated_runs_overlap_velocity_copy():
         vel = w.vel if i % 2 == 0 else w.vel.copy()  # a fresh host buffer every other run
         cat = plan.run(w.pos, vel, members=True)
         assert_same_catalog(cat, ref)
+
+
+def test_graph_replay_after_an_eager_run_of_another_shape():
+    """Run A is recorded in a graph; run B (another linking length) is issued
+    eagerly with graphs off, which replaces the device's box table; A replayed
+    afterwards must use A's table again."""
+    import torch
+    w = synth.config2(seed=401, scale=30000 / 256 ** 3)
+    dev = torch.device("cuda", 0)
+    pos, vel = torch.from_numpy(w.pos).to(dev), torch.from_numpy(w.vel).to(dev)
+    cfg_a = FofConfig.from_workload(w)
+    cfg_b = FofConfig.from_workload(w)
+    cfg_b.linklength = 1.3 * w.linklength
+    ref_a = cpu.run(w)
+    plan = Plan(cfg_a)
+    try:
+        for _ in range(2):
+            assert_same_catalog(plan.run(pos, vel, members=True), ref_a)
+        plan.set_graph(False)
+        plan.set_config(cfg_b)
+        cat_b = plan.run(pos, vel, members=True)
+        # the longer length gathers more particles into the halos
+        assert cat_b.props[:, 0].sum() > ref_a["halo_props"][:, 0].sum()
+        plan.set_graph(True)
+        plan.set_config(cfg_a)
+        for _ in range(2):
+            assert_same_catalog(plan.run(pos, vel, members=True), ref_a)
+    finally:
+        plan.close()

@@ -22,7 +22,9 @@ shrinks any of them.
 Timing: CUDA events on the launching stream, W untimed warm-up steps, K timed
 steps between barriers + synchronize; inputs (400 MB) exceed L2.
 `e2e` repeats the measurement through the public API with pinned host
-inputs: host->device copy, the run, and the catalog read back.
+inputs: every step copies its inputs host->device inside the timed region
+(the copy of step i + 1 is started before step i runs and overlaps it:
+Plan.prefetch), runs, and reads its catalog back.
 """
 from __future__ import annotations
 
@@ -269,16 +271,29 @@ def run_ours(args):
     plan.set_graph(not args.no_graph)
     if tune is not None:
         plan.set_tuning(tune)
-    for _ in range(max(1, args.warmup)):
-        plan.run(pin_pos, pin_vel, out="host", stream=stream)
+    # a second input buffer does not fit beside the 1024^3 box's workspace
+    ahead = args.config != "c5"
+
+    def e2e_steps(k):
+        # every step's inputs are copied from pinned host memory; the copy of
+        # step i + 1 is started (prefetch) before step i runs, so that it
+        # overlaps step i's work on the GPU
+        nbytes = 0
+        if ahead:
+            plan.prefetch(pin_pos, pin_vel, stream=stream)
+        for i in range(k):
+            if ahead and i + 1 < k:
+                plan.prefetch(pin_pos, pin_vel, stream=stream)
+            hc = plan.run(pin_pos, pin_vel, out="host", stream=stream)
+            nbytes = hc.props.nbytes + hc.head.nbytes
+        return nbytes
+
+    e2e_steps(max(3, args.warmup))
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    d2h = 0
-    for _ in range(args.steps):
-        hc = plan.run(pin_pos, pin_vel, out="host", stream=stream)
-        d2h = hc.props.nbytes + hc.head.nbytes
+    d2h = e2e_steps(args.steps)
     e1.record(stream)
     barrier()
     plan.close()

@@ -219,6 +219,18 @@ class Plan:
         finally:
             self._L.cmh_catalog_free(C.byref(cat))
 
+    def prefetch(self, pos, vel, stream=None):
+        """Start copying host (numpy, ideally pinned) arrays to the device
+        ahead of a later run(pos, vel) with the same arrays, so that the
+        copy overlaps the GPU's current work (cmh_plan_prefetch)."""
+        if not (pos.flags.c_contiguous and vel.flags.c_contiguous):
+            raise ValueError("host arrays must be C-contiguous")
+        parts = _abi.Particles(n=int(pos.shape[0]), pos_dtype=_dtype_code(pos),
+                               vel_dtype=_dtype_code(vel), pos=pos.ctypes.data,
+                               vel=vel.ctypes.data, id=None, location=CMH_HOST)
+        _abi.check(self._L.cmh_plan_prefetch(self._h, C.byref(parts),
+                                             C.c_void_p(self._stream(stream))))
+
     def set_graph(self, enable: bool):
         """Replay runs of a repeated shape from a captured CUDA graph."""
         _abi.check(self._L.cmh_plan_set_graph(self._h, int(bool(enable))))

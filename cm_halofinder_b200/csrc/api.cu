@@ -108,11 +108,16 @@ Plan::Plan(const cmh_fof_params &p, int pdt, int dev) : device(dev), pos_dtype(p
 
 Plan::~Plan() {
   cudaSetDevice(device);
-  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  for (cudaGraphExec_t g : graph_exec)
+    if (g) cudaGraphExecDestroy(g);
+  if (side_stream) cudaStreamSynchronize(side_stream);
   if (cap_stream) cudaStreamDestroy(cap_stream);
   if (side_stream) cudaStreamDestroy(side_stream);
   if (ev_side_start) cudaEventDestroy(ev_side_start);
-  if (ev_vel_ready) cudaEventDestroy(ev_vel_ready);
+  for (int b = 0; b < 2; b++) {
+    if (ev_pos[b]) cudaEventDestroy(ev_pos[b]);
+    if (ev_vel[b]) cudaEventDestroy(ev_vel[b]);
+  }
   each_buf([](DevBuf &b) { b.release(); });
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -122,9 +127,13 @@ Plan::~Plan() {
 
 void Plan::release_workspace() {
   cudaSetDevice(device);
-  if (graph_exec) cudaGraphExecDestroy(graph_exec);
-  graph_exec = nullptr;
-  graph_sig.clear();
+  for (int q = 0; q < 2; q++) {
+    if (graph_exec[q]) cudaGraphExecDestroy(graph_exec[q]);
+    graph_exec[q] = nullptr;
+    graph_sig[q].clear();
+  }
+  if (side_stream) cudaStreamSynchronize(side_stream);
+  staged.clear();
   uploaded_sig.clear();
   each_buf([](DevBuf &b) { b.release(); });
   np_cap = nd_cap = nc_cap = 0;
@@ -310,31 +319,9 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog 
   memset(cat, 0, sizeof *cat);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cmh_particles dp = *parts;
-  if (parts->location == CMH_HOST && parts->n > 0) {
-    // host particles: copied into plan-owned device buffers on the stream
-    CMH_CUDA(cudaSetDevice(pl.device));
-    const size_t pb = (size_t)parts->n * 3 * (parts->pos_dtype == CMH_FLOAT64 ? 8 : 4);
-    const size_t vb = (size_t)parts->n * 3 * (parts->vel_dtype == CMH_FLOAT64 ? 8 : 4);
-    pl.in_pos.ensure(pb);
-    pl.in_vel.ensure(vb);
-    if (!pl.side_stream) {
-      CMH_CUDA(cudaStreamCreateWithFlags(&pl.side_stream, cudaStreamNonBlocking));
-      CMH_CUDA(cudaEventCreateWithFlags(&pl.ev_side_start, cudaEventDisableTiming));
-      CMH_CUDA(cudaEventCreateWithFlags(&pl.ev_vel_ready, cudaEventDisableTiming));
-    }
-    // positions on the caller's stream; velocities on the side stream once
-    // the caller's earlier work (the previous run's sums read in_vel) is done
-    CMH_CUDA(cudaEventRecord(pl.ev_side_start, s));
-    CMH_CUDA(cudaStreamWaitEvent(pl.side_stream, pl.ev_side_start, 0));
-    CMH_CUDA(cudaMemcpyAsync(pl.in_pos.p, parts->pos, pb, cudaMemcpyHostToDevice, s));
-    CMH_CUDA(cudaMemcpyAsync(pl.in_vel.p, parts->vel, vb, cudaMemcpyHostToDevice,
-                             pl.side_stream));
-    CMH_CUDA(cudaEventRecord(pl.ev_vel_ready, pl.side_stream));
-    pl.vel_wait = true;
-    dp.pos = pl.in_pos.p;
-    dp.vel = pl.in_vel.p;
-    dp.location = CMH_DEVICE;
-  }
+  // host particles: copied into plan-owned device buffers on the plan's side
+  // stream (or already being copied, by cmh_plan_prefetch)
+  if (parts->location == CMH_HOST && parts->n > 0) dp = pl.take_inputs(*parts, s);
   struct Reset {
     Plan &p;
     ~Reset() { p.vel_wait = false; }
@@ -342,6 +329,26 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog 
   pl.run(dp, want_member != 0, s);
   if (out_location == CMH_DEVICE) catalog_on_device(pl, cat, want_member != 0);
   else catalog_to_host(pl, cat, want_member != 0, 0, s);
+  CMH_API_END
+}
+
+cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *stream) {
+  CMH_API_BEGIN
+  if (!plan) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan is required");
+  check_parts(parts);
+  Plan &pl = *static_cast<Plan *>(plan);
+  if (parts->location != CMH_HOST)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "only host-resident particles are copied ahead");
+  if (parts->pos_dtype != pl.pos_dtype)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "position dtype differs from the plan's");
+  if (pl.staged.size() >= 2)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "two runs are staged already");
+  if (parts->n == 0) return CMH_OK;
+  // the buffer that neither the last run nor the newest staged inputs hold
+  const int b = pl.stage_inputs(*parts, static_cast<cudaStream_t>(stream),
+                                1 - (pl.staged.empty() ? pl.last_buf : pl.staged.back().buf));
+  pl.staged.push_back(cmh::Plan::Staged{parts->pos, parts->vel, parts->n, parts->pos_dtype,
+                                        parts->vel_dtype, b});
   CMH_API_END
 }
 

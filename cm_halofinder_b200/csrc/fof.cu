@@ -2185,7 +2185,10 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     });
     sig.insert(sig.end(), (const unsigned char *)ltab_all.data(),
                (const unsigned char *)(ltab_all.data() + ltab_all.size()));
-    const bool same = graph_exec && sig == graph_sig;
+    int slot = -1;  // the recorded graph of this shape, if any
+    for (int q = 0; q < 2; q++)
+      if (graph_exec[q] && sig == graph_sig[q]) slot = q;
+    const bool same = slot >= 0;
     // the device box table (and length tables) hold the last uploaded shape,
     // which an eager run of another shape may have replaced since the graph
     // was recorded: upload whenever they differ from this run's
@@ -2203,7 +2206,8 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
     if (use_graph && same) {
       // a replay is timed as a whole; stage times come from eager runs
       CMH_CUDA(cudaEventRecord(ev0, s));
-      CMH_CUDA(cudaGraphLaunch(graph_exec, s));
+      CMH_CUDA(cudaGraphLaunch(graph_exec[slot], s));
+      graph_next = 1 - slot;  // keep the one just used
       CMH_CUDA(cudaEventRecord(ev1, s));
       launches_per_run_graph_ok = true;
       read_back(s, false);
@@ -2226,9 +2230,12 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
 }
 
 void Plan::capture(bool want_member, cudaStream_t s, const std::vector<unsigned char> &sig) {
-  if (graph_exec) {
-    cudaGraphExecDestroy(graph_exec);
-    graph_exec = nullptr;
+  const int q = graph_next;
+  graph_next = 1 - q;
+  if (graph_exec[q]) {
+    cudaGraphExecDestroy(graph_exec[q]);
+    graph_exec[q] = nullptr;
+    graph_sig[q].clear();
   }
   // recorded on the plan's own stream (the legacy stream cannot be
   // captured); the graph is then launched on the caller's stream
@@ -2244,10 +2251,10 @@ void Plan::capture(bool want_member, cudaStream_t s, const std::vector<unsigned 
     throw;
   }
   CMH_CUDA(cudaStreamEndCapture(cap_stream, &graph));
-  cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
+  cudaError_t e = cudaGraphInstantiate(&graph_exec[q], graph, 0);
   cudaGraphDestroy(graph);
   CMH_CUDA(e);
-  graph_sig = sig;
+  graph_sig[q] = sig;
   (void)s;
 }
 
@@ -2296,6 +2303,59 @@ cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaSt
   cell_scale = best.cell_scale;
   dense_min = (uint32_t)best.dense_min;
   return best;
+}
+
+int Plan::stage_inputs(const cmh_particles &parts, cudaStream_t s, int b) {
+  CMH_CUDA(cudaSetDevice(device));
+  if (!side_stream) {
+    CMH_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_side_start, cudaEventDisableTiming));
+    for (int b = 0; b < 2; b++) {
+      CMH_CUDA(cudaEventCreateWithFlags(&ev_pos[b], cudaEventDisableTiming));
+      CMH_CUDA(cudaEventCreateWithFlags(&ev_vel[b], cudaEventDisableTiming));
+    }
+  }
+  const size_t pb = (size_t)parts.n * 3 * (parts.pos_dtype == CMH_FLOAT64 ? 8 : 4);
+  const size_t vb = (size_t)parts.n * 3 * (parts.vel_dtype == CMH_FLOAT64 ? 8 : 4);
+  in_pos[b].ensure(pb);
+  in_vel[b].ensure(vb);
+  // after the caller's queued work (a run that read this buffer before), on
+  // the side stream: the positions first, at the link's full bandwidth
+  CMH_CUDA(cudaEventRecord(ev_side_start, s));
+  CMH_CUDA(cudaStreamWaitEvent(side_stream, ev_side_start, 0));
+  CMH_CUDA(cudaMemcpyAsync(in_pos[b].p, parts.pos, pb, cudaMemcpyHostToDevice, side_stream));
+  CMH_CUDA(cudaEventRecord(ev_pos[b], side_stream));
+  CMH_CUDA(cudaMemcpyAsync(in_vel[b].p, parts.vel, vb, cudaMemcpyHostToDevice, side_stream));
+  CMH_CUDA(cudaEventRecord(ev_vel[b], side_stream));
+  return b;
+}
+
+cmh_particles Plan::take_inputs(const cmh_particles &parts, cudaStream_t s) {
+  int b = -1;
+  if (!staged.empty()) {
+    const Staged &f = staged.front();
+    if (f.pos == parts.pos && f.vel == parts.vel && f.n == parts.n &&
+        f.pos_dtype == parts.pos_dtype && f.vel_dtype == parts.vel_dtype) {
+      b = f.buf;
+      staged.erase(staged.begin());
+    } else {
+      // not what was staged: the staged copies are dropped
+      CMH_CUDA(cudaStreamSynchronize(side_stream));
+      staged.clear();
+    }
+  }
+  // not staged: copied now, into the first buffer (a plan that is never
+  // given prefetches keeps a single input buffer)
+  if (b < 0) b = stage_inputs(parts, s, 0);
+  last_buf = b;
+  CMH_CUDA(cudaStreamWaitEvent(s, ev_pos[b], 0));
+  ev_vel_ready = ev_vel[b];
+  vel_wait = true;
+  cmh_particles dp = parts;
+  dp.pos = in_pos[b].p;
+  dp.vel = in_vel[b].p;
+  dp.location = CMH_DEVICE;
+  return dp;
 }
 
 void Plan::run(const cmh_particles &parts, bool want_member, cudaStream_t s) {

@@ -57,15 +57,29 @@ struct Plan : public cmh_plan {
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t stage_ev[7] = {};  // boundaries between the eight stages
-  cudaGraphExec_t graph_exec = nullptr;
-  std::vector<unsigned char> graph_sig;
+  // the recorded graphs of the last two run shapes (two, so that runs that
+  // alternate between the two host-input buffers both replay)
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  std::vector<unsigned char> graph_sig[2];
+  int graph_next = 0;  // the slot the next recording replaces
   std::vector<unsigned char> uploaded_sig;  // shape whose box table is on the device
   cudaStream_t cap_stream = nullptr;  // the stream runs are recorded on
-  // host-resident inputs: velocities are copied on a side stream while the
-  // run's first stages go on, and the property sums wait for them
+  // host-resident inputs: copied into one of two device buffers on a side
+  // stream, positions first; a run waits for its positions before it starts
+  // and for its velocities before the property sums (which are the first to
+  // read them).  cmh_plan_prefetch stages the next run's inputs into the other
+  // buffer while a run computes.
   cudaStream_t side_stream = nullptr;
-  cudaEvent_t ev_side_start = nullptr, ev_vel_ready = nullptr;
+  cudaEvent_t ev_side_start = nullptr, ev_pos[2] = {}, ev_vel[2] = {};
+  cudaEvent_t ev_vel_ready = nullptr;  // the current run's (one of ev_vel)
   bool vel_wait = false;
+  struct Staged {
+    const void *pos, *vel;
+    int64_t n;
+    int pos_dtype, vel_dtype, buf;
+  };
+  std::vector<Staged> staged;  // inputs being copied ahead, oldest first (at most 2)
+  int last_buf = 0;            // the buffer of the last run's inputs
   // subsampling of the run's particles (FOF.c:205-284): rates, seed and the
   // particle IDs on the device (NULL: the input index is the key)
   bool sampling = false;
@@ -82,7 +96,7 @@ struct Plan : public cmh_plan {
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;
   DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
-  DevBuf in_pos, in_vel;  // device copies of host-resident particles
+  DevBuf in_pos[2], in_vel[2];  // device copies of host-resident particles
   DevBuf b_samp;          // per input particle: 0, 1 (kept, in a halo), 2 (kept, outside)
 
   // every workspace buffer, for release and for the graph signature
@@ -94,7 +108,7 @@ struct Plan : public cmh_plan {
                      &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
                      &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
                      &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
-                     &in_pos, &in_vel, &b_samp};
+                     &in_pos[0], &in_vel[0], &in_pos[1], &in_vel[1], &b_samp};
     for (DevBuf *b : all) f(*b);
   }
   void release_workspace();
@@ -112,6 +126,11 @@ struct Plan : public cmh_plan {
   void run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaStream_t s);
   cmh_tuning autotune(const std::vector<BoxSpec> &specs, int repeats, cudaStream_t s);
   void run(const cmh_particles &parts, bool want_member, cudaStream_t s);
+  // host inputs: start copying them into the next input buffer (after the
+  // caller's queued work), returning the buffer; take the staged inputs that
+  // match `parts` (or copy them now) and return the device description
+  int stage_inputs(const cmh_particles &parts, cudaStream_t s, int buf);
+  cmh_particles take_inputs(const cmh_particles &parts, cudaStream_t s);
 };
 
 }  // namespace cmh

@@ -191,6 +191,20 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts,
                         cmh_catalog *cat, int32_t want_member,
                         int32_t out_location, void *stream);
 
+/* Starts copying host-resident particles (parts->location == CMH_HOST) into
+ * plan-owned device memory on a stream of the plan's own, after the work
+ * already queued on `stream`, so that the copy overlaps whatever the GPU is
+ * doing -- typically the previous run.  A later cmh_plan_run given the same
+ * host arrays (same pointers, count and dtypes) uses the staged copy instead
+ * of copying again; a run given other host arrays drops what was staged.  At
+ * most two runs can be staged ahead (CMH_ERR_INVALID_ARGUMENT beyond).  The
+ * host arrays must stay unchanged until that run returns, and be pinned for
+ * the copy to overlap.  Without a prefetch, cmh_plan_run copies host inputs
+ * itself the same way: positions first, the velocities while the run's first
+ * stages go on.  The reference reads its particles before FOF() (Read_Data,
+ * read_data.c:100-404); nothing there overlaps. */
+cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *stream);
+
 /* Changes the run parameters of a plan (same precision of positions). */
 cmh_status cmh_plan_set_params(cmh_plan *plan, const cmh_fof_params *params);
 

@@ -3,6 +3,8 @@ rerun path, against the CPU oracle box by box."""
 import numpy as np
 import pytest
 
+import cm_halofinder_b200 as cmh
+
 from cm_halofinder_b200 import FofConfig, Plan, fof, synth
 from oracle import cpu
 from tests.helpers import assert_same_catalog
@@ -140,5 +142,37 @@ def test_graph_replay_after_an_eager_run_of_another_shape():
         plan.set_config(cfg_a)
         for _ in range(2):
             assert_same_catalog(plan.run(pos, vel, members=True), ref_a)
+    finally:
+        plan.close()
+
+
+def test_prefetched_host_inputs():
+    """Host inputs copied ahead with prefetch(): each run uses the copy staged
+    for its arrays (one step ahead, alternating between the plan's two input
+    buffers and their two recorded graphs); a run given other arrays drops
+    what was staged; a third pending prefetch is refused."""
+    import torch
+    ws = [synth.config2(seed=420 + i, scale=25000 / 256 ** 3) for i in range(2)]
+    refs = [cpu.run(w) for w in ws]
+    host = [(torch.from_numpy(w.pos).pin_memory().numpy(),
+             torch.from_numpy(w.vel).pin_memory().numpy()) for w in ws]
+    plan = Plan(FofConfig.from_workload(ws[0]))
+    try:
+        order = [0, 0, 0, 0, 0]
+        plan.prefetch(*host[order[0]])
+        for i, k in enumerate(order):
+            if i + 1 < len(order):
+                plan.prefetch(*host[order[i + 1]])
+            assert_same_catalog(plan.run(*host[k], members=True), refs[k])
+        # staged for box 0, run on box 1: the staged copy is dropped
+        plan.set_config(FofConfig.from_workload(ws[1]))
+        plan.prefetch(*host[0])
+        assert_same_catalog(plan.run(*host[1], members=True), refs[1])
+        plan.prefetch(*host[1])
+        plan.prefetch(*host[1])
+        with pytest.raises(cmh.CmhError):
+            plan.prefetch(*host[1])
+        for _ in range(2):
+            assert_same_catalog(plan.run(*host[1], members=True), refs[1])
     finally:
         plan.close()

@@ -230,6 +230,11 @@ def run_ours(args):
     value = n_all / (ms * 1e-3) / 1e6
     cat_fast = plan.run(pos, vel, out="host", stream=stream)
     plan.close()
+    cpu_boxes = None
+    if args.config == "c5" and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference's sample sub-domains, cut on the device while the
+        # box is there (its host copy is not kept)
+        cpu_boxes = subbox_sample(DeviceBox(w, pos, vel), subbox_split(n), 24)
 
     plain = None
     if not args.no_plain and args.precision != "fp64":
@@ -326,12 +331,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        if args.config == "c5":
-            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                   "sample": "not run for the 1024^3 box (the sampled sub-domains of the "
-                             "256^3 box give the reference's rate)"}
-        else:
-            cpu = cpu_baseline(w, args.cpu_seconds)
+        cpu = cpu_baseline(w, args.cpu_seconds, boxes=cpu_boxes)
     rep.close()
     if rank != 0:
         return
@@ -478,21 +478,46 @@ def run_batched(args):
     }), flush=True)
 
 
-def cpu_baseline(w, seconds, ndiv=16, timeout=None, procs=1, seed=0):
+class DeviceBox:
+    """A workload's run parameters with its particles as device tensors."""
+
+    def __init__(self, w, pos, vel):
+        self.__dict__.update({k: v for k, v in vars(w).items() if k not in ("pos", "vel")})
+        self.pos, self.vel = pos, vel
+
+
+def subbox_split(n):
+    """Ranks per axis of the reference's domain split for a CPU sample: about
+    4096 particles per rank's domain (16^3 for the 256^3 box)."""
+    return max(1, int(round((n / 4096) ** (1.0 / 3.0))))
+
+
+def subbox_sample(w, ndiv, count, seed=0):
+    """The first `count` sub-domains of a seeded order of the ndiv^3 split."""
+    from oracle import reference
+    order = np.random.default_rng(seed).permutation(ndiv ** 3)
+    return [reference.SubBox(w, ndiv, int(i)) for i in order[:count]]
+
+
+def cpu_baseline(w, seconds, ndiv=None, timeout=None, procs=1, seed=0, boxes=None):
     """The reference's own FoF (oracle/_ref) on host cores, on sub-boxes of
-    the same box (one rank's domain of an ndiv^3 decomposition each)."""
+    the same box (one rank's domain of an ndiv^3 decomposition each, or the
+    given ones)."""
     from oracle import reference
     if not reference.available("cmh_ref_f32_timing"):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "reference binary not built (oracle/_ref missing)"}
+    if ndiv is None:
+        ndiv = subbox_split(w.n)
     rng = np.random.default_rng(seed)
     order = rng.permutation(ndiv ** 3)
     timeout = timeout or max(5.0, seconds / 2)
     done_n, spent, ok, to = 0, 0.0, 0, 0
     t_end = time.perf_counter() + seconds
     k = 0
-    while time.perf_counter() < t_end and k < len(order):
-        sb = reference.SubBox(w, ndiv, int(order[k]))
+    limit = len(boxes) if boxes is not None else len(order)
+    while time.perf_counter() < t_end and k < limit:
+        sb = boxes[k] if boxes is not None else reference.SubBox(w, ndiv, int(order[k]))
         k += 1
         dt, wall = reference.time_subbox(sb, timeout=min(timeout, max(1.0, t_end - time.perf_counter() + 1)))
         spent += wall
@@ -502,11 +527,15 @@ def cpu_baseline(w, seconds, ndiv=16, timeout=None, procs=1, seed=0):
             ok += 1
             done_n += sb.n_owned
     value = done_n / spent / 1e6 if spent > 0 else None
+    note = ""
+    if getattr(w, "varlink", None):
+        note = ("; the reference's variable linking length does not compile (VARLINK), so it "
+                f"runs with the constant l = {w.linklength:.4f}, the table's largest value")
     return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
             "sample": f"{ok} of {ndiv}^3 sub-box domains (one rank each, ghost shell "
-                      f"{w.boundary}) of this box run to completion, {to} stopped at the "
-                      f"per-domain time limit and counted with zero particles; "
-                      f"{spent:.1f} s of one core"}
+                      f"{w.boundary}{'' if w.periodic else ', no periodic wrap'}) of this "
+                      f"box run to completion, {to} stopped at the per-domain time limit and "
+                      f"counted with zero particles; {spent:.1f} s of one core" + note}
 
 
 def _ref_worker(argv):
@@ -533,7 +562,7 @@ def run_reference(args):
     import pickle
     w = make_workload(args, 0)
     cores = os.cpu_count() or 1
-    ndiv = 16
+    ndiv = subbox_split(w.n)
     order = np.random.default_rng(0).permutation(ndiv ** 3)
     blob = pickle.dumps(w)
     ctx = mp.get_context("spawn")

@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ cells,
 
 // Grid cell and linking length of every processed particle (variable
 // linking length runs only; boxes with a fixed length get cell 0 and their
-// own l^2 / band, which reproduces the fixed-length test).
+// own l^2, which reproduces the fixed-length test).
 template <class PT, bool FP32>
 __global__ void __launch_bounds__(kT) k_varlink_recs(const SPos<PT> *__restrict__ spos,
                                                      const uint32_t *__restrict__ run_of,
@@ -445,22 +445,12 @@ __global__ void __launch_bounds__(kT) k_varlink_recs(const SPos<PT> *__restrict_
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const Geom &g = boxes[run_box[run_of[i]]].g;
     VLRec<FP32> v;
-    double lsq = g.linksq;
     v.rkey = 0;
+    v.lsq = g.linksq;
     if (g.varlink) {
       const SPos<PT> p = spos[i];
       v.rkey = ref_key(g, (double)p.x, (double)p.y, (double)p.z);
-      lsq = ref_cell_linksq(g, v.rkey);
-    }
-    if constexpr (FP32) {
-      if (g.varlink) {
-        band_thresholds(lsq, sizeof(PT) == 4 ? 4 : 8, &v.t_lo, &v.t_hi);
-      } else {
-        v.t_lo = g.t_lo;
-        v.t_hi = g.t_hi;
-      }
-    } else {
-      v.lsq = lsq;
+      v.lsq = ref_cell_linksq(g, v.rkey);
     }
     svl[i] = v;
   }
@@ -565,17 +555,10 @@ __device__ __forceinline__ bool linked(const SPos<PT> &p, const SPos<PT> &q, con
                                        unsigned long long &rechecks) {
   float t_lo = g.t_lo, t_hi = g.t_hi;
   double lsq = g.linksq;
-  uint64_t rk = 0;
   if constexpr (VL) {
     if (!ref_neighbours(va.rkey, vb.rkey)) return false;
-    const VLRec<FP32> &v = va.rkey <= vb.rkey ? va : vb;
-    rk = v.rkey;
-    if constexpr (FP32) {
-      t_lo = v.t_lo;
-      t_hi = v.t_hi;
-    } else {
-      lsq = v.lsq;
-    }
+    lsq = (va.rkey <= vb.rkey ? va : vb).lsq;
+    if constexpr (FP32) vl_band(lsq, sizeof(PT) == 4 ? 4 : 8, &t_lo, &t_hi);
   }
   double dx, dy, dz;
   if constexpr (sizeof(PT) == 4) {
@@ -602,7 +585,6 @@ __device__ __forceinline__ bool linked(const SPos<PT> &p, const SPos<PT> &q, con
       rechecks++;
     }
   }
-  if constexpr (VL && FP32) lsq = g.varlink ? ref_cell_linksq(g, rk) : g.linksq;
   const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
   return !(d2 > lsq);
 }
@@ -1793,7 +1775,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     if (fp32)
       k_varlink_recs<PT, true><<<rg(k_varlink_recs<PT, true>, npc), kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
                                                  b_run_box.as<uint16_t>(), boxes, sc,
-                                                 b_svl.as<VLRec32>());
+                                                 b_svl.as<VLRec64>());
     else
       k_varlink_recs<PT, false><<<rg(k_varlink_recs<PT, false>, npc), kT, 0, s>>>(b_spos.as<SPos<PT>>(), run_of,
                                                   b_run_box.as<uint16_t>(), boxes, sc,

@@ -124,19 +124,30 @@ __host__ __device__ inline void band_thresholds(double l2, int ulps, float *t_lo
 // cell scans itself and its 13 forward neighbours (FOF.c:111-153).  Pairs
 // whose cells are not neighbours are never tested.  Each processed particle
 // therefore carries its grid cell (packed z << 42 | y << 21 | x, which
-// orders like the scan) and that cell's l^2 (plain FP64 form) or FP32 band
-// (FP32 form; the band re-check recomputes l^2 from the cell).
+// orders like the scan) and that cell's l^2; the FP32 form derives its band
+// from that l^2 (vl_band below).
 struct __align__(16) VLRec64 {
   uint64_t rkey;
   double lsq;
 };
-struct __align__(16) VLRec32 {
-  uint64_t rkey;
-  float t_lo, t_hi;
-};
-template <bool FP32> struct VLRecOf { using type = VLRec64; };
-template <> struct VLRecOf<true> { using type = VLRec32; };
-template <bool FP32> using VLRec = typename VLRecOf<FP32>::type;
+template <bool FP32> using VLRec = VLRec64;
+
+// The FP32 band around a variable l^2 from the bits of fl32(l^2): from
+// 2 ulps steps below to ulps steps above.  A step below fl32(l^2) is at
+// least half its spacing (less only across a power of two), so the band
+// holds at least `ulps` spacings on each side -- the band of
+// band_thresholds(), which is the one the proof needs.  A subnormal or zero
+// fl32(l^2) sends every pair to the double test.
+__device__ __forceinline__ void vl_band(double lsq, int ulps, float *t_lo, float *t_hi) {
+  const uint32_t b = __float_as_uint(__double2float_rn(lsq));
+  if (b < 0x00800000u) {
+    *t_lo = -1.0f;
+    *t_hi = __int_as_float(0x7f800000);
+    return;
+  }
+  *t_lo = __uint_as_float(b - 2u * (uint32_t)ulps);
+  *t_hi = __uint_as_float(b + (uint32_t)ulps);
+}
 
 // Cell of the fixed grid holding (x, y, z): floor((x - rmin_buff) / lcell)
 // per axis, in double with IEEE division (FOF.c:76-92).

@@ -113,9 +113,13 @@ def read_catalog(path, halosize):
 
 class SubBox:
     """One rank's domain of the reference's Nx = Ny = Nz = ndiv decomposition
-    of a periodic box (startup.c:33-47), with its ghost shell filled by the
-    periodic wrap the reference applies to received ghosts
-    (read_data.c:792-797).  Used to time the reference on bounded samples."""
+    of a box (startup.c:33-47) with its ghost shell: for a periodic box the
+    shell is filled by the periodic wrap the reference applies to received
+    ghosts (read_data.c:792-797); for an isolated domain (a lightcone) the
+    shell holds the particles within Boundarysize of the sub-domain, with no
+    wrap.  Used to time the reference on bounded samples.  `w.pos` / `w.vel`
+    may be numpy arrays or torch tensors on a GPU (the cut is then made
+    there and only the sub-domain's particles are copied to the host)."""
 
     def __init__(self, w, ndiv, index):
         L = w.hi[0] - w.lo[0]
@@ -123,12 +127,33 @@ class SubBox:
         ix, iy, iz = index % ndiv, (index // ndiv) % ndiv, index // (ndiv * ndiv)
         lo = np.array([w.lo[0] + ix * side, w.lo[1] + iy * side, w.lo[2] + iz * side])
         b = w.boundary
-        x = w.pos.astype(np.float64)
-        y = np.mod(x - (lo - b), L)            # offset from the padded low corner
-        keep = np.all(y <= side + 2 * b, axis=1)
-        self.ppos = (lo - b + y[keep]).astype(w.pos.dtype)
-        self.pvel = w.vel[keep]
-        self.n_owned = int(np.all((y[keep] >= b) & (y[keep] < side + b), axis=1).sum())
+        if not isinstance(w.pos, np.ndarray):
+            import torch
+            x = w.pos
+            off = torch.tensor(lo - b, dtype=torch.float64, device=x.device)
+            keep = torch.ones(x.shape[0], dtype=torch.bool, device=x.device)
+            for a in range(3):  # per axis, to bound the temporaries
+                y = x[:, a].double() - off[a]
+                if w.periodic:
+                    y = torch.remainder(y, L)
+                keep &= (y >= 0) & (y <= side + 2 * b)
+            idx = torch.nonzero(keep).squeeze(1)
+            y = x[idx].double() - off
+            if w.periodic:
+                y = torch.remainder(y, L)
+            y = y.cpu().numpy()
+            self.pvel = w.vel[idx].cpu().numpy()
+            dtype = np.float32 if x.dtype == torch.float32 else np.float64
+        else:
+            y = w.pos.astype(np.float64) - (lo - b)  # offset from the padded low corner
+            if w.periodic:
+                y = np.mod(y, L)
+            keep = np.all((y >= 0) & (y <= side + 2 * b), axis=1)
+            y = y[keep]
+            self.pvel = w.vel[keep]
+            dtype = w.pos.dtype
+        self.ppos = (lo - b + y).astype(dtype)
+        self.n_owned = int(np.all((y >= b) & (y < side + b), axis=1).sum())
         self.lo = tuple(lo)
         self.hi = tuple(lo + side)
         self.boundary = b

@@ -103,3 +103,32 @@ def test_reference_binary_links_the_same_pairs(dtype):
     linked_pairs = sorted(int(h["ids"].min()) // 2 for h in halos)
     assert all(h["ids"].shape[0] == 2 for h in halos)
     assert linked_pairs == [i for i, (_, l64, _) in enumerate(cases) if l64]
+
+
+def vl_band(lsq, ulps):
+    """The kernels' band for a variable l^2 (vl_band in fof_kernels.cuh):
+    from 2 ulps float steps below fl32(l^2) to ulps steps above."""
+    b = int(np.array([lsq], np.float32).view(np.uint32)[0])
+    lo = np.array([b - 2 * ulps], np.uint32).view(np.float32)[0]
+    hi = np.array([b + ulps], np.uint32).view(np.float32)[0]
+    return Fraction(float(lo)), Fraction(float(hi))
+
+
+@pytest.mark.parametrize("ulps", [4, 8])
+def test_variable_length_band_contains_the_proven_band(ulps):
+    """Whatever fl32(l^2) is -- inside a binade or just above a power of two,
+    where the steps below are half as wide -- the band derived from its bits
+    contains band_thresholds()'s, so the proof covers it."""
+    rng = np.random.default_rng(7 + ulps)
+    vals = list(10 ** rng.uniform(-6, 4, 3000))
+    for e in range(-20, 14):  # at and just around powers of two
+        for d in (-3, -1, 0, 1, 2, 5, 9):
+            vals.append(float(np.nextafter(np.float32(2.0 ** e), np.float32(np.inf)) * 1.0)
+                        + d * 2.0 ** (e - 23))
+    for v in vals:
+        if v <= 0:
+            continue
+        l2d = f64(Fraction(v))
+        lo, hi = vl_band(float(l2d), ulps)
+        rlo, rhi = band(l2d, ulps)
+        assert lo <= rlo and hi >= rhi, (v, lo, rlo, hi, rhi)

@@ -1147,6 +1147,9 @@ __global__ void __launch_bounds__(kT, 4) k_befriend(
         bx2 = l_x0 + (int)(sl % (uint32_t)l_nx);
         by2 = l_y0 + (int)((sl / (uint32_t)l_nx) % (uint32_t)l_ny);
         bz2 = l_z0 + (int)(sl / (uint32_t)(l_nx * l_ny));
+        // a slot of the other phase is dropped before its row is read
+        const int cheb_s = max(abs(bx2 - gx), max(abs(by2 - gy), abs(bz2 - gz)));
+        if ((PHASE == 0 && cheb_s > 1) || (PHASE == 1 && cheb_s <= 1)) continue;
         // occupancy bit of the slot's fine cell, then its index from the
         // top cell's row prefix (fine cells are in sub-cell order)
         const uint32_t *gr = grows + (uint64_t)l_map * 2 * kk;

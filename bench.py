@@ -437,19 +437,31 @@ def run_batched(args):
                  "speedup_of_chosen_form": ms_p / ms}
         plan_p.close()
 
-    # end to end: pinned host inputs copied in every step, catalogs read back
-    hpos = [torch.from_numpy(w.pos).pin_memory() for w in boxes]
-    hvel = [torch.from_numpy(w.vel).pin_memory() for w in boxes]
-    dpos = [torch.empty_like(p, device=dev) for p in hpos]
-    dvel = [torch.empty_like(v, device=dev) for v in hvel]
+    # end to end: the boxes' pinned host arrays given to run_batch, which
+    # copies them to the device in every step; the copy of step i + 1 is
+    # started (prefetch_batch) before step i runs, so that it overlaps step
+    # i's work on the GPU; catalogs read back
+    hpos = [torch.from_numpy(w.pos).pin_memory().numpy() for w in boxes]
+    hvel = [torch.from_numpy(w.vel).pin_memory().numpy() for w in boxes]
 
-    def copied():
-        for a, b in zip(dpos + dvel, hpos + hvel):
-            a.copy_(b, non_blocking=True)
-        return dpos, dvel
+    def e2e_steps(k):
+        plan.prefetch_batch(hpos, hvel, stream=stream)
+        for i in range(k):
+            if i + 1 < k:
+                plan.prefetch_batch(hpos, hvel, stream=stream)
+            out = plan.run_batch(cfgs, hpos, hvel, stream=stream)
+        return out
 
-    ms_e2e, _, _ = timed(plan, args.steps, max(1, args.warmup), copied)
-    d2h = sum(c.props.nbytes + c.head.nbytes for c in cats)
+    e2e_steps(max(3, args.warmup))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cats_e2e = e2e_steps(args.steps)
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_ranks(e0.elapsed_time(e1) / args.steps)
+    d2h = sum(c.props.nbytes + c.head.nbytes for c in cats_e2e)
     e2e = {"value": n_all / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": int(sum(w.pos.nbytes + w.vel.nbytes for w in boxes)),
            "d2h_bytes_per_step": int(d2h)}

@@ -235,17 +235,41 @@ class Plan:
         """Replay runs of a repeated shape from a captured CUDA graph."""
         _abi.check(self._L.cmh_plan_set_graph(self._h, int(bool(enable))))
 
+    def _parts(self, positions, velocities):
+        """Particle descriptions of the boxes: torch CUDA tensors (device) or
+        C-contiguous numpy arrays (host)."""
+        nb = len(positions)
+        parts = (_abi.Particles * nb)()
+        for b in range(nb):
+            pos, vel = positions[b], velocities[b]
+            if isinstance(pos, np.ndarray) != isinstance(vel, np.ndarray):
+                raise ValueError("a box's positions and velocities are both numpy "
+                                 "(host) or both torch tensors (device)")
+            if isinstance(pos, np.ndarray):
+                if not (pos.flags.c_contiguous and vel.flags.c_contiguous):
+                    raise ValueError("host arrays must be C-contiguous")
+                parts[b] = _abi.Particles(n=int(pos.shape[0]), pos_dtype=_dtype_code(pos),
+                                          vel_dtype=_dtype_code(vel), pos=pos.ctypes.data,
+                                          vel=vel.ctypes.data, id=None, location=CMH_HOST)
+            else:
+                parts[b] = _abi.Particles(n=int(pos.shape[0]), pos_dtype=self._tdt(pos),
+                                          vel_dtype=self._tdt(vel), pos=self._ptr(pos),
+                                          vel=self._ptr(vel), id=None, location=CMH_DEVICE)
+        return parts
+
     def _batch_args(self, configs, positions, velocities):
         nb = len(configs)
         cs = [c.to_c() for c in configs]     # keep the varlink tables alive
         P = (_abi.FofParams * nb)(*cs)
-        parts = (_abi.Particles * nb)()
-        for b in range(nb):
-            pos, vel = positions[b], velocities[b]
-            parts[b] = _abi.Particles(n=int(pos.shape[0]), pos_dtype=self._tdt(pos),
-                                      vel_dtype=self._tdt(vel), pos=self._ptr(pos),
-                                      vel=self._ptr(vel), id=None, location=CMH_DEVICE)
-        return nb, P, parts, cs
+        return nb, P, self._parts(positions, velocities), cs
+
+    def prefetch_batch(self, positions, velocities, stream=None):
+        """Start copying the host (numpy, ideally pinned) arrays of a later
+        run_batch with the same boxes, in the same order, to the device
+        (cmh_plan_prefetch_batch)."""
+        parts = self._parts(positions, velocities)
+        _abi.check(self._L.cmh_plan_prefetch_batch(self._h, parts, len(positions),
+                                                   C.c_void_p(self._stream(stream))))
 
     @staticmethod
     def _stream(stream):
@@ -272,7 +296,9 @@ class Plan:
     def run_batch(self, configs, positions, velocities, stream=None, with_status=False):
         """Many independent boxes in one run (one sort, one befriending pass,
         one reduction for all of them); positions/velocities are torch CUDA
-        tensors.  Returns one host Catalog per box.  with_status: each box is
+        tensors, or numpy arrays for every box (copied to the device inside
+        the call, or taken from prefetch_batch).  Returns one host Catalog
+        per box.  with_status: each box is
         checked on its own (cmh_plan_run_batch_status) and (catalogs,
         statuses) is returned, a rejected box's catalog being None."""
         nb, P, parts, _keep = self._batch_args(configs, positions, velocities)

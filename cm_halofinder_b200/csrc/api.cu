@@ -321,7 +321,7 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog 
   cmh_particles dp = *parts;
   // host particles: copied into plan-owned device buffers on the plan's side
   // stream (or already being copied, by cmh_plan_prefetch)
-  if (parts->location == CMH_HOST && parts->n > 0) dp = pl.take_inputs(*parts, s);
+  if (parts->location == CMH_HOST && parts->n > 0) dp = pl.take_inputs(parts, 1, s)[0];
   struct Reset {
     Plan &p;
     ~Reset() { p.vel_wait = false; }
@@ -332,23 +332,41 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts, cmh_catalog 
   CMH_API_END
 }
 
-cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *stream) {
-  CMH_API_BEGIN
-  if (!plan) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan is required");
-  check_parts(parts);
-  Plan &pl = *static_cast<Plan *>(plan);
-  if (parts->location != CMH_HOST)
-    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "only host-resident particles are copied ahead");
-  if (parts->pos_dtype != pl.pos_dtype)
-    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "position dtype differs from the plan's");
+namespace {
+void prefetch_on(Plan &pl, const cmh_particles *parts, int32_t nbox, void *stream) {
+  int64_t total = 0;
+  for (int b = 0; b < nbox; b++) {
+    check_parts(&parts[b]);
+    if (parts[b].location != CMH_HOST)
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "only host-resident particles are copied ahead");
+    if (parts[b].pos_dtype != pl.pos_dtype)
+      cmh::fail(CMH_ERR_INVALID_ARGUMENT, "position dtype differs from the plan's");
+    total += parts[b].n;
+  }
   if (pl.staged.size() >= 2)
     cmh::fail(CMH_ERR_INVALID_ARGUMENT, "two runs are staged already");
-  if (parts->n == 0) return CMH_OK;
+  if (total == 0) return;
   // the buffer that neither the last run nor the newest staged inputs hold
-  const int b = pl.stage_inputs(*parts, static_cast<cudaStream_t>(stream),
+  const int b = pl.stage_inputs(parts, nbox, static_cast<cudaStream_t>(stream),
                                 1 - (pl.staged.empty() ? pl.last_buf : pl.staged.back().buf));
-  pl.staged.push_back(cmh::Plan::Staged{parts->pos, parts->vel, parts->n, parts->pos_dtype,
-                                        parts->vel_dtype, b});
+  pl.staged.push_back(
+      cmh::Plan::Staged{std::vector<cmh_particles>(parts, parts + nbox), b});
+}
+}  // namespace
+
+cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *stream) {
+  CMH_API_BEGIN
+  if (!plan || !parts) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and particles are required");
+  prefetch_on(*static_cast<Plan *>(plan), parts, 1, stream);
+  CMH_API_END
+}
+
+cmh_status cmh_plan_prefetch_batch(cmh_plan *plan, const cmh_particles *parts, int32_t nbox,
+                                   void *stream) {
+  CMH_API_BEGIN
+  if (!plan || !parts || nbox < 1)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and particles are required");
+  prefetch_on(*static_cast<Plan *>(plan), parts, nbox, stream);
   CMH_API_END
 }
 
@@ -516,8 +534,37 @@ std::vector<cmh::BoxSpec> make_specs(Plan &pl, const cmh_fof_params *params,
   return specs;
 }
 
+// Host-resident boxes (all of a batch, or none) are copied into the plan's
+// input buffers first, or taken from a prefetch of the same boxes.
 void run_batch_on(Plan &pl, const cmh_fof_params *params, const cmh_particles *parts,
                   int32_t nbox, cmh_catalog *cats, cudaStream_t s) {
+  int host = 0;
+  int64_t total = 0;
+  for (int b = 0; b < nbox; b++) {
+    check_parts(&parts[b]);
+    host += parts[b].location == CMH_HOST;
+    total += parts[b].n;
+  }
+  if (host != 0 && host != nbox)
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT,
+              "a batch's boxes are all host-resident or all device-resident");
+  std::vector<cmh_particles> dp;
+  if (host) {
+    for (int b = 0; b < nbox; b++)
+      if (parts[b].pos_dtype != pl.pos_dtype)
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "all boxes of a batch share the position dtype");
+    if (total > 0) {
+      dp = pl.take_inputs(parts, nbox, s);
+    } else {
+      dp.assign(parts, parts + nbox);
+      for (cmh_particles &q : dp) q.location = CMH_DEVICE;  // nothing to read
+    }
+    parts = dp.data();
+  }
+  struct Reset {
+    Plan &p;
+    ~Reset() { p.vel_wait = false; }
+  } reset{pl};
   pl.run_batch(make_specs(pl, params, parts, nbox), false, s);
   for (int b = 0; b < nbox; b++) catalog_to_host(pl, &cats[b], false, b, s);
 }
@@ -589,8 +636,9 @@ cmh_status cmh_plan_run_batch_status(cmh_plan *plan, const cmh_fof_params *param
     box_status[b] = CMH_OK;
     try {
       check_parts(&parts[b]);
-      if (parts[b].location != CMH_DEVICE)
-        cmh::fail(CMH_ERR_INVALID_ARGUMENT, "batched runs take device-resident particles");
+      if (parts[b].location != parts[0].location)
+        cmh::fail(CMH_ERR_INVALID_ARGUMENT,
+                  "a batch's boxes are all host-resident or all device-resident");
       if (parts[b].pos_dtype != pl.pos_dtype)
         cmh::fail(CMH_ERR_INVALID_ARGUMENT, "position dtype differs from the plan's");
       const cmh_fof_params &p = params[b];

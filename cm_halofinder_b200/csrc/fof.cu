@@ -2290,7 +2290,35 @@ cmh_tuning Plan::autotune(const std::vector<BoxSpec> &specs, int repeats, cudaSt
   return best;
 }
 
-int Plan::stage_inputs(const cmh_particles &parts, cudaStream_t s, int b) {
+namespace {
+// Byte offsets of each box's positions and velocities in the input buffers
+// (256-byte aligned slices); returns the totals.
+void input_layout(const cmh_particles *parts, int nbox, std::vector<size_t> *opos,
+                  std::vector<size_t> *ovel, size_t *tpos, size_t *tvel) {
+  size_t p = 0, v = 0;
+  opos->resize(nbox);
+  ovel->resize(nbox);
+  for (int i = 0; i < nbox; i++) {
+    (*opos)[i] = p;
+    (*ovel)[i] = v;
+    p += ((size_t)parts[i].n * 3 * (parts[i].pos_dtype == CMH_FLOAT64 ? 8 : 4) + 255) & ~(size_t)255;
+    v += ((size_t)parts[i].n * 3 * (parts[i].vel_dtype == CMH_FLOAT64 ? 8 : 4) + 255) & ~(size_t)255;
+  }
+  *tpos = p;
+  *tvel = v;
+}
+
+bool same_inputs(const std::vector<cmh_particles> &a, const cmh_particles *b, int nbox) {
+  if ((int)a.size() != nbox) return false;
+  for (int i = 0; i < nbox; i++)
+    if (a[i].pos != b[i].pos || a[i].vel != b[i].vel || a[i].n != b[i].n ||
+        a[i].pos_dtype != b[i].pos_dtype || a[i].vel_dtype != b[i].vel_dtype)
+      return false;
+  return true;
+}
+}  // namespace
+
+int Plan::stage_inputs(const cmh_particles *parts, int nbox, cudaStream_t s, int b) {
   CMH_CUDA(cudaSetDevice(device));
   if (!side_stream) {
     CMH_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
@@ -2300,27 +2328,36 @@ int Plan::stage_inputs(const cmh_particles &parts, cudaStream_t s, int b) {
       CMH_CUDA(cudaEventCreateWithFlags(&ev_vel[b], cudaEventDisableTiming));
     }
   }
-  const size_t pb = (size_t)parts.n * 3 * (parts.pos_dtype == CMH_FLOAT64 ? 8 : 4);
-  const size_t vb = (size_t)parts.n * 3 * (parts.vel_dtype == CMH_FLOAT64 ? 8 : 4);
-  in_pos[b].ensure(pb);
-  in_vel[b].ensure(vb);
+  std::vector<size_t> opos, ovel;
+  size_t tpos, tvel;
+  input_layout(parts, nbox, &opos, &ovel, &tpos, &tvel);
+  in_pos[b].ensure(std::max<size_t>(tpos, 256));
+  in_vel[b].ensure(std::max<size_t>(tvel, 256));
   // after the caller's queued work (a run that read this buffer before), on
   // the side stream: the positions first, at the link's full bandwidth
   CMH_CUDA(cudaEventRecord(ev_side_start, s));
   CMH_CUDA(cudaStreamWaitEvent(side_stream, ev_side_start, 0));
-  CMH_CUDA(cudaMemcpyAsync(in_pos[b].p, parts.pos, pb, cudaMemcpyHostToDevice, side_stream));
+  for (int i = 0; i < nbox; i++)
+    if (parts[i].n > 0)
+      CMH_CUDA(cudaMemcpyAsync(in_pos[b].as<unsigned char>() + opos[i], parts[i].pos,
+                               (size_t)parts[i].n * 3 * (parts[i].pos_dtype == CMH_FLOAT64 ? 8 : 4),
+                               cudaMemcpyHostToDevice, side_stream));
   CMH_CUDA(cudaEventRecord(ev_pos[b], side_stream));
-  CMH_CUDA(cudaMemcpyAsync(in_vel[b].p, parts.vel, vb, cudaMemcpyHostToDevice, side_stream));
+  for (int i = 0; i < nbox; i++)
+    if (parts[i].n > 0)
+      CMH_CUDA(cudaMemcpyAsync(in_vel[b].as<unsigned char>() + ovel[i], parts[i].vel,
+                               (size_t)parts[i].n * 3 * (parts[i].vel_dtype == CMH_FLOAT64 ? 8 : 4),
+                               cudaMemcpyHostToDevice, side_stream));
   CMH_CUDA(cudaEventRecord(ev_vel[b], side_stream));
   return b;
 }
 
-cmh_particles Plan::take_inputs(const cmh_particles &parts, cudaStream_t s) {
+std::vector<cmh_particles> Plan::take_inputs(const cmh_particles *parts, int nbox,
+                                             cudaStream_t s) {
   int b = -1;
   if (!staged.empty()) {
     const Staged &f = staged.front();
-    if (f.pos == parts.pos && f.vel == parts.vel && f.n == parts.n &&
-        f.pos_dtype == parts.pos_dtype && f.vel_dtype == parts.vel_dtype) {
+    if (same_inputs(f.parts, parts, nbox)) {
       b = f.buf;
       staged.erase(staged.begin());
     } else {
@@ -2331,15 +2368,20 @@ cmh_particles Plan::take_inputs(const cmh_particles &parts, cudaStream_t s) {
   }
   // not staged: copied now, into the first buffer (a plan that is never
   // given prefetches keeps a single input buffer)
-  if (b < 0) b = stage_inputs(parts, s, 0);
+  if (b < 0) b = stage_inputs(parts, nbox, s, 0);
   last_buf = b;
   CMH_CUDA(cudaStreamWaitEvent(s, ev_pos[b], 0));
   ev_vel_ready = ev_vel[b];
   vel_wait = true;
-  cmh_particles dp = parts;
-  dp.pos = in_pos[b].p;
-  dp.vel = in_vel[b].p;
-  dp.location = CMH_DEVICE;
+  std::vector<size_t> opos, ovel;
+  size_t tpos, tvel;
+  input_layout(parts, nbox, &opos, &ovel, &tpos, &tvel);
+  std::vector<cmh_particles> dp(parts, parts + nbox);
+  for (int i = 0; i < nbox; i++) {
+    dp[i].pos = in_pos[b].as<unsigned char>() + opos[i];
+    dp[i].vel = in_vel[b].as<unsigned char>() + ovel[i];
+    dp[i].location = CMH_DEVICE;
+  }
   return dp;
 }
 

@@ -74,9 +74,8 @@ struct Plan : public cmh_plan {
   cudaEvent_t ev_vel_ready = nullptr;  // the current run's (one of ev_vel)
   bool vel_wait = false;
   struct Staged {
-    const void *pos, *vel;
-    int64_t n;
-    int pos_dtype, vel_dtype, buf;
+    std::vector<cmh_particles> parts;  // the host inputs as given, one per box
+    int buf;
   };
   std::vector<Staged> staged;  // inputs being copied ahead, oldest first (at most 2)
   int last_buf = 0;            // the buffer of the last run's inputs
@@ -126,11 +125,12 @@ struct Plan : public cmh_plan {
   void run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaStream_t s);
   cmh_tuning autotune(const std::vector<BoxSpec> &specs, int repeats, cudaStream_t s);
   void run(const cmh_particles &parts, bool want_member, cudaStream_t s);
-  // host inputs: start copying them into the next input buffer (after the
-  // caller's queued work), returning the buffer; take the staged inputs that
-  // match `parts` (or copy them now) and return the device description
-  int stage_inputs(const cmh_particles &parts, cudaStream_t s, int buf);
-  cmh_particles take_inputs(const cmh_particles &parts, cudaStream_t s);
+  // host inputs of nbox boxes: start copying them into input buffer `buf`
+  // (after the caller's queued work; every box's positions before any
+  // velocities), returning the buffer; take the staged inputs that match
+  // `parts` (or copy them now) and return the device descriptions
+  int stage_inputs(const cmh_particles *parts, int nbox, cudaStream_t s, int buf);
+  std::vector<cmh_particles> take_inputs(const cmh_particles *parts, int nbox, cudaStream_t s);
 };
 
 }  // namespace cmh

@@ -205,6 +205,13 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts,
  * read_data.c:100-404); nothing there overlaps. */
 cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *stream);
 
+/* cmh_plan_prefetch for the `nbox` host-resident boxes of a later
+ * cmh_plan_run_batch (or cmh_plan_run_batch_status) given the same boxes in
+ * the same order: every box's positions are copied before any velocities.
+ * No reference counterpart (the reference runs one domain per rank). */
+cmh_status cmh_plan_prefetch_batch(cmh_plan *plan, const cmh_particles *parts, int32_t nbox,
+                                   void *stream);
+
 /* Changes the run parameters of a plan (same precision of positions). */
 cmh_status cmh_plan_set_params(cmh_plan *plan, const cmh_fof_params *params);
 
@@ -234,7 +241,9 @@ cmh_status cmh_plan_autotune(cmh_plan *plan, const cmh_fof_params *params,
 cmh_status cmh_plan_set_tuning(cmh_plan *plan, const cmh_tuning *tuning);
 
 /* cmh_fof_run_batch on a plan: repeated batches of the same shape replay one
- * CUDA graph.  Any box's error fails the whole call. */
+ * CUDA graph.  Any box's error fails the whole call.  The boxes may also be
+ * all host-resident: they are then copied into plan-owned device memory as
+ * for cmh_plan_run (or taken from cmh_plan_prefetch_batch). */
 cmh_status cmh_plan_run_batch(cmh_plan *plan, const cmh_fof_params *params,
                               const cmh_particles *parts, int32_t nbox, cmh_catalog *cats,
                               void *stream);

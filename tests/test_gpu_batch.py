@@ -176,3 +176,40 @@ def test_prefetched_host_inputs():
             assert_same_catalog(plan.run(*host[1], members=True), refs[1])
     finally:
         plan.close()
+
+
+def test_host_batch_with_prefetch():
+    """A batch of host-resident boxes: copied inside the call, or staged one
+    step ahead with prefetch_batch (both input buffers in turn); every box
+    matches the oracle.  A batch mixing host and device boxes is refused."""
+    import torch
+    boxes = _boxes(5, 9)
+    refs = [cpu.run(w) for w in boxes]
+    cfgs = [FofConfig.from_workload(w) for w in boxes]
+    hpos = [torch.from_numpy(w.pos).pin_memory().numpy() for w in boxes]
+    hvel = [torch.from_numpy(w.vel).pin_memory().numpy() for w in boxes]
+    plan = Plan(cfgs[0])
+    try:
+        def check(cats):
+            for cat, ref in zip(cats, refs):
+                assert_same_catalog(cat, ref, check_member=False)
+        check(plan.run_batch(cfgs, hpos, hvel))          # copied in the call
+        plan.prefetch_batch(hpos, hvel)
+        for i in range(4):
+            if i + 1 < 4:
+                plan.prefetch_batch(hpos, hvel)
+            check(plan.run_batch(cfgs, hpos, hvel))
+        # staged for these boxes, run on a subset: the staged copy is dropped
+        plan.prefetch_batch(hpos, hvel)
+        cats = plan.run_batch(cfgs[:3], hpos[:3], hvel[:3])
+        for cat, ref in zip(cats, refs[:3]):
+            assert_same_catalog(cat, ref, check_member=False)
+        mpos = [torch.from_numpy(boxes[0].pos).cuda()] + hpos[1:]
+        mvel = [torch.from_numpy(boxes[0].vel).cuda()] + hvel[1:]
+        with pytest.raises(cmh.CmhError) as e:
+            plan.run_batch(cfgs, mpos, mvel)
+        assert e.value.status == 1
+        with pytest.raises(ValueError):
+            plan.run_batch(cfgs, mpos, hvel)
+    finally:
+        plan.close()

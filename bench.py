@@ -129,9 +129,10 @@ def describe(args, w, dtype, n):
             f"{w.meta['n_clumps']} clumps, l={w.linklength:.6f}, Boundarysize={w.boundary}")
 
 
-# DRAM bytes per processed particle of the befriending launches (ncu, 256^3
-# box at scale 1/2: 444.5 MB for 8,971,801 processed particles)
-BEFRIEND_DRAM_PER_PROC = 444.50e6 / 8971801
+# DRAM bytes per processed particle of the befriending launches (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of the stage's six launches,
+# 256^3 box at scale 1/2: 431.9 MB for 8,971,801 processed particles)
+BEFRIEND_DRAM_PER_PROC = 431.88e6 / 8971801
 
 # the launches behind each stage's CUDA-event interval
 KERNELS = {
@@ -316,9 +317,8 @@ def run_ours(args):
         # DRAM bytes of the befriending launches per processed particle, from
         # an ncu capture of the 256^3 box at scale 1/2
         traffic = int(BEFRIEND_DRAM_PER_PROC * st["n_proc"])
-        traffic_src = ("ncu dram__bytes.sum (read + write: dram__bytes.sum.per_second x "
-                       "gpu__time_duration.sum) of the stage's six launches on the 256^3 box at "
-                       "scale 1/2, scaled by processed particles")
+        traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the stage's six "
+                       "launches on the 256^3 box at scale 1/2, scaled by processed particles")
     roofline = {"bound": "hbm", "kernel": KERNELS.get(dominant, dominant),
                 "achieved": round(ach, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",

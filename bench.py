@@ -277,18 +277,20 @@ def run_ours(args):
     plan.set_graph(not args.no_graph)
     if tune is not None:
         plan.set_tuning(tune)
-    # a second input buffer does not fit beside the 1024^3 box's workspace
-    ahead = args.config != "c5"
+    # a second input buffer does not fit beside the 1024^3 box's workspace:
+    # there the next step's copies go into the same buffer once this step
+    # has read it (positions after ingest, velocities after the sums)
+    if args.config == "c5":
+        plan.set_input_buffers(1)
 
     def e2e_steps(k):
         # every step's inputs are copied from pinned host memory; the copy of
         # step i + 1 is started (prefetch) before step i runs, so that it
         # overlaps step i's work on the GPU
         nbytes = 0
-        if ahead:
-            plan.prefetch(pin_pos, pin_vel, stream=stream)
+        plan.prefetch(pin_pos, pin_vel, stream=stream)
         for i in range(k):
-            if ahead and i + 1 < k:
+            if i + 1 < k:
                 plan.prefetch(pin_pos, pin_vel, stream=stream)
             hc = plan.run(pin_pos, pin_vel, out="host", stream=stream)
             nbytes = hc.props.nbytes + hc.head.nbytes
@@ -331,12 +333,14 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w, args.cpu_seconds, boxes=cpu_boxes)
+        cpu = cpu_baseline(w, args.cpu_seconds, boxes=cpu_boxes,
+                           ndiv=subbox_split(n) if cpu_boxes is not None else None)
     rep.close()
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "metric": METRIC.replace("256^3", "1024^3") if args.config == "c5" else METRIC,
+        "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64-recheck" if args.precision == "fp32" else "f64",
@@ -519,10 +523,10 @@ def cpu_baseline(w, seconds, ndiv=None, timeout=None, procs=1, seed=0, boxes=Non
     if not reference.available("cmh_ref_f32_timing"):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "reference binary not built (oracle/_ref missing)"}
-    if ndiv is None:
-        ndiv = subbox_split(w.n)
-    rng = np.random.default_rng(seed)
-    order = rng.permutation(ndiv ** 3)
+    if boxes is None:
+        if ndiv is None:
+            ndiv = subbox_split(w.n)
+        order = np.random.default_rng(seed).permutation(ndiv ** 3)
     timeout = timeout or max(5.0, seconds / 2)
     done_n, spent, ok, to = 0, 0.0, 0, 0
     t_end = time.perf_counter() + seconds

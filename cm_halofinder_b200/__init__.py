@@ -231,6 +231,13 @@ class Plan:
         _abi.check(self._L.cmh_plan_prefetch(self._h, C.byref(parts),
                                              C.c_void_p(self._stream(stream))))
 
+    def set_input_buffers(self, n: int):
+        """Device copies of host inputs the plan keeps: 2 (default) or 1, for
+        workspaces that leave no room for a second (cmh_plan_set_input_buffers);
+        with 1, prefetch() copies into the same buffer once the current run
+        has read it."""
+        _abi.check(self._L.cmh_plan_set_input_buffers(self._h, int(n)))
+
     def set_graph(self, enable: bool):
         """Replay runs of a repeated shape from a captured CUDA graph."""
         _abi.check(self._L.cmh_plan_set_graph(self._h, int(bool(enable))))

@@ -136,6 +136,7 @@ SIGNATURES = {
     "cmh_plan_prefetch": (C.c_int, [C.c_void_p, C.POINTER(Particles), C.c_void_p]),
     "cmh_plan_prefetch_batch": (C.c_int, [C.c_void_p, C.POINTER(Particles), C.c_int32,
                                           C.c_void_p]),
+    "cmh_plan_set_input_buffers": (C.c_int, [C.c_void_p, C.c_int32]),
     "cmh_fof_labels_noalloc": (C.c_int, [C.POINTER(FofParams), C.c_void_p, C.c_int32,
                                          C.c_int64, C.c_void_p, C.c_void_p]),
     "cmh_read_parameterfile": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(RunParameters)]),

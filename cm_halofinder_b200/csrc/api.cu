@@ -114,6 +114,8 @@ Plan::~Plan() {
   if (cap_stream) cudaStreamDestroy(cap_stream);
   if (side_stream) cudaStreamDestroy(side_stream);
   if (ev_side_start) cudaEventDestroy(ev_side_start);
+  if (ev_pos_free) cudaEventDestroy(ev_pos_free);
+  if (ev_vel_free) cudaEventDestroy(ev_vel_free);
   for (int b = 0; b < 2; b++) {
     if (ev_pos[b]) cudaEventDestroy(ev_pos[b]);
     if (ev_vel[b]) cudaEventDestroy(ev_vel[b]);
@@ -346,11 +348,22 @@ void prefetch_on(Plan &pl, const cmh_particles *parts, int32_t nbox, void *strea
   if (pl.staged.size() >= 2)
     cmh::fail(CMH_ERR_INVALID_ARGUMENT, "two runs are staged already");
   if (total == 0) return;
+  std::vector<cmh_particles> v(parts, parts + nbox);
+  if (pl.input_buffers == 1) {
+    // one buffer: copied now if it holds nothing that a later run needs,
+    // else behind the next run's reads of it
+    if (pl.staged.empty()) {
+      pl.stage_inputs(parts, nbox, static_cast<cudaStream_t>(stream), 0);
+      pl.staged.push_back(cmh::Plan::Staged{v, 0, false});
+    } else {
+      pl.staged.push_back(cmh::Plan::Staged{v, 0, true});
+    }
+    return;
+  }
   // the buffer that neither the last run nor the newest staged inputs hold
   const int b = pl.stage_inputs(parts, nbox, static_cast<cudaStream_t>(stream),
                                 1 - (pl.staged.empty() ? pl.last_buf : pl.staged.back().buf));
-  pl.staged.push_back(
-      cmh::Plan::Staged{std::vector<cmh_particles>(parts, parts + nbox), b});
+  pl.staged.push_back(cmh::Plan::Staged{v, b, false});
 }
 }  // namespace
 
@@ -358,6 +371,23 @@ cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *s
   CMH_API_BEGIN
   if (!plan || !parts) cmh::fail(CMH_ERR_INVALID_ARGUMENT, "plan and particles are required");
   prefetch_on(*static_cast<Plan *>(plan), parts, 1, stream);
+  CMH_API_END
+}
+
+cmh_status cmh_plan_set_input_buffers(cmh_plan *plan, int32_t n) {
+  CMH_API_BEGIN
+  if (!plan || (n != 1 && n != 2))
+    cmh::fail(CMH_ERR_INVALID_ARGUMENT, "a plan and 1 or 2 input buffers are required");
+  Plan &pl = *static_cast<Plan *>(plan);
+  CMH_CUDA(cudaSetDevice(pl.device));
+  if (pl.side_stream) CMH_CUDA(cudaStreamSynchronize(pl.side_stream));
+  pl.staged.clear();  // staged copies are dropped
+  pl.input_buffers = n;
+  pl.last_buf = 0;
+  if (n == 1) {
+    pl.in_pos[1].release();
+    pl.in_vel[1].release();
+  }
   CMH_API_END
 }
 

@@ -1691,6 +1691,19 @@ int64_t rows_cap_for(int64_t np_cap, uint64_t k3all) {
   return (int64_t)(((uint64_t)np_cap * 4 + (1ull << 30)) / (rows_per_top(k3all) * 8));
 }
 
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CMH_CUDA(cudaStreamIsCapturing(s, &cs));
+  return cs == cudaStreamCaptureStatusActive;
+}
+
+// An event record that other streams can wait on also when it is replayed
+// from a recorded graph.
+void record_external(cudaEvent_t e, cudaStream_t s) {
+  if (capturing(s)) CMH_CUDA(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
+  else CMH_CUDA(cudaEventRecord(e, s));
+}
+
 // Images per input particle expected for a periodic box (the shell's share
 // of the padded volume), with headroom for clustering.
 double image_estimate(const Geom &g, int64_t n) {
@@ -1751,6 +1764,9 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_LAUNCHED();
   }
   mark(0);
+  // host inputs: their positions are read no more (a next run's may be
+  // copied into their buffer)
+  if (vel_wait) record_external(ev_pos_free, s);
   // ---- sort ----
   // the sort leaves the indices in cell order in b_vals and no sorted keys:
   // k_gather_flags recomputes the fine cells into b_keys from the positions
@@ -1881,11 +1897,8 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   if (vel_wait) {
     // host-resident velocities arrive on the side stream while the steps
     // above run; the sums are their first reader
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    CMH_CUDA(cudaStreamIsCapturing(s, &cs));
     CMH_CUDA(cudaStreamWaitEvent(s, ev_vel_ready,
-                                 cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal
-                                                                     : cudaEventWaitDefault));
+                                 capturing(s) ? cudaEventWaitExternal : cudaEventWaitDefault));
   }
   const int NS = 6 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
   CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, s));
@@ -1902,6 +1915,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 #undef CMH_SUMS
   CMH_LAUNCHED();
   mark(5);
+  if (vel_wait) record_external(ev_vel_free, s);  // nor their velocities
 #define CMH_OWNED(NSV)                                                                          \
   k_owned<NSV><<<rg(k_owned<NSV>, ncc), kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),              \
                                  b_count.as<uint32_t>(), b_run_box.as<uint16_t>(), boxes, sc, \
@@ -2148,6 +2162,7 @@ void Plan::read_back(cudaStream_t s, bool timed) {
 
 void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaStream_t s) {
   CMH_CUDA(cudaSetDevice(device));
+  overwritten = false;
   for (int attempt = 0; attempt < 3; attempt++) {
     prepare(specs, want_member);
     // the graph stays valid while the inputs, sizes and capacities do
@@ -2195,11 +2210,13 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
       graph_next = 1 - slot;  // keep the one just used
       CMH_CUDA(cudaEventRecord(ev1, s));
       launches_per_run_graph_ok = true;
+      queue_pending();
       read_back(s, false);
       CMH_CUDA(cudaEventElapsedTime(&stats.ms_total, ev0, ev1));
     } else {
       if (pos_dtype == CMH_FLOAT64) issue<double>(want_member, s, true);
       else issue<float>(want_member, s, true);
+      queue_pending();
       read_back(s, true);
       launches_per_run = (int32_t)(g_launches - l0);
       if (!(last.overflow & 1u) && use_graph) capture(want_member, s, sig);
@@ -2210,6 +2227,16 @@ void Plan::run_batch(const std::vector<BoxSpec> &specs, bool want_member, cudaSt
                                  std::max<int64_t>(nd_cap, rows_cap_for(np_cap, k3all)));
     if (!(last.overflow & 1u)) return;
     np_cap = (int64_t)last.np_raw + last.np_raw / 8 + 4096;  // repeat with room
+    if (overwritten) {
+      // one input buffer, already refilled with the next run's inputs: this
+      // run's are copied again, and the next run's wait for the repeat
+      CMH_CUDA(cudaStreamSynchronize(side_stream));
+      staged.front().pending = true;
+      overwritten = false;
+      stage_inputs(cur_host.data(), (int)cur_host.size(), s, 0);
+      CMH_CUDA(cudaStreamWaitEvent(s, ev_pos[0], 0));
+      ev_vel_ready = ev_vel[0];
+    }
   }
   fail(CMH_ERR_CAPACITY, "processed particles kept outgrowing the buffers");
 }
@@ -2318,16 +2345,21 @@ bool same_inputs(const std::vector<cmh_particles> &a, const cmh_particles *b, in
 }
 }  // namespace
 
+void Plan::ensure_side() {
+  if (side_stream) return;
+  CMH_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
+  CMH_CUDA(cudaEventCreateWithFlags(&ev_side_start, cudaEventDisableTiming));
+  CMH_CUDA(cudaEventCreateWithFlags(&ev_pos_free, cudaEventDisableTiming));
+  CMH_CUDA(cudaEventCreateWithFlags(&ev_vel_free, cudaEventDisableTiming));
+  for (int b = 0; b < 2; b++) {
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_pos[b], cudaEventDisableTiming));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_vel[b], cudaEventDisableTiming));
+  }
+}
+
 int Plan::stage_inputs(const cmh_particles *parts, int nbox, cudaStream_t s, int b) {
   CMH_CUDA(cudaSetDevice(device));
-  if (!side_stream) {
-    CMH_CUDA(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
-    CMH_CUDA(cudaEventCreateWithFlags(&ev_side_start, cudaEventDisableTiming));
-    for (int b = 0; b < 2; b++) {
-      CMH_CUDA(cudaEventCreateWithFlags(&ev_pos[b], cudaEventDisableTiming));
-      CMH_CUDA(cudaEventCreateWithFlags(&ev_vel[b], cudaEventDisableTiming));
-    }
-  }
+  ensure_side();
   std::vector<size_t> opos, ovel;
   size_t tpos, tvel;
   input_layout(parts, nbox, &opos, &ovel, &tpos, &tvel);
@@ -2337,28 +2369,56 @@ int Plan::stage_inputs(const cmh_particles *parts, int nbox, cudaStream_t s, int
   // the side stream: the positions first, at the link's full bandwidth
   CMH_CUDA(cudaEventRecord(ev_side_start, s));
   CMH_CUDA(cudaStreamWaitEvent(side_stream, ev_side_start, 0));
+  copy_inputs(parts, nbox, b, false);
+  return b;
+}
+
+// The copies of staged host inputs into buffer b on the side stream, every
+// box's positions before any velocities.  `behind_run`: the positions wait
+// for the queued run's ingest and the velocities for its property sums.
+void Plan::copy_inputs(const cmh_particles *parts, int nbox, int b, bool behind_run) {
+  std::vector<size_t> opos, ovel;
+  size_t tpos, tvel;
+  input_layout(parts, nbox, &opos, &ovel, &tpos, &tvel);
+  if (behind_run) CMH_CUDA(cudaStreamWaitEvent(side_stream, ev_pos_free, 0));
   for (int i = 0; i < nbox; i++)
     if (parts[i].n > 0)
       CMH_CUDA(cudaMemcpyAsync(in_pos[b].as<unsigned char>() + opos[i], parts[i].pos,
                                (size_t)parts[i].n * 3 * (parts[i].pos_dtype == CMH_FLOAT64 ? 8 : 4),
                                cudaMemcpyHostToDevice, side_stream));
   CMH_CUDA(cudaEventRecord(ev_pos[b], side_stream));
+  if (behind_run) CMH_CUDA(cudaStreamWaitEvent(side_stream, ev_vel_free, 0));
   for (int i = 0; i < nbox; i++)
     if (parts[i].n > 0)
       CMH_CUDA(cudaMemcpyAsync(in_vel[b].as<unsigned char>() + ovel[i], parts[i].vel,
                                (size_t)parts[i].n * 3 * (parts[i].vel_dtype == CMH_FLOAT64 ? 8 : 4),
                                cudaMemcpyHostToDevice, side_stream));
   CMH_CUDA(cudaEventRecord(ev_vel[b], side_stream));
-  return b;
+}
+
+void Plan::queue_pending() {
+  if (input_buffers != 1 || staged.empty() || !staged.front().pending) return;
+  Staged &f = staged.front();
+  std::vector<size_t> opos, ovel;
+  size_t tpos, tvel;
+  input_layout(f.parts.data(), (int)f.parts.size(), &opos, &ovel, &tpos, &tvel);
+  // the buffer is in use by the queued run: it is not grown now (a larger
+  // next run is copied when it starts)
+  if (tpos > in_pos[0].cap || tvel > in_vel[0].cap) return;
+  copy_inputs(f.parts.data(), (int)f.parts.size(), 0, true);
+  f.pending = false;
+  overwritten = true;
 }
 
 std::vector<cmh_particles> Plan::take_inputs(const cmh_particles *parts, int nbox,
                                              cudaStream_t s) {
   int b = -1;
+  cur_host.assign(parts, parts + nbox);
+  overwritten = false;
   if (!staged.empty()) {
     const Staged &f = staged.front();
     if (same_inputs(f.parts, parts, nbox)) {
-      b = f.buf;
+      if (!f.pending) b = f.buf;  // else copied now, below
       staged.erase(staged.begin());
     } else {
       // not what was staged: the staged copies are dropped

@@ -68,17 +68,25 @@ struct Plan : public cmh_plan {
   // stream, positions first; a run waits for its positions before it starts
   // and for its velocities before the property sums (which are the first to
   // read them).  cmh_plan_prefetch stages the next run's inputs into the other
-  // buffer while a run computes.
+  // buffer while a run computes.  With one input buffer (input_buffers == 1)
+  // the next run's copies go into the same buffer once the current run is
+  // done with it: its positions after the current run's ingest (ev_pos_free)
+  // and its velocities after its property sums (ev_vel_free).
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_side_start = nullptr, ev_pos[2] = {}, ev_vel[2] = {};
+  cudaEvent_t ev_pos_free = nullptr, ev_vel_free = nullptr;
   cudaEvent_t ev_vel_ready = nullptr;  // the current run's (one of ev_vel)
   bool vel_wait = false;
+  int input_buffers = 2;
   struct Staged {
     std::vector<cmh_particles> parts;  // the host inputs as given, one per box
     int buf;
+    bool pending;  // one-buffer mode: not copied yet (waits for the run before)
   };
   std::vector<Staged> staged;  // inputs being copied ahead, oldest first (at most 2)
   int last_buf = 0;            // the buffer of the last run's inputs
+  std::vector<cmh_particles> cur_host;  // host inputs of the run in progress
+  bool overwritten = false;    // one-buffer mode: the next run's copies were queued
   // subsampling of the run's particles (FOF.c:205-284): rates, seed and the
   // particle IDs on the device (NULL: the input index is the key)
   bool sampling = false;
@@ -131,6 +139,11 @@ struct Plan : public cmh_plan {
   // `parts` (or copy them now) and return the device descriptions
   int stage_inputs(const cmh_particles *parts, int nbox, cudaStream_t s, int buf);
   std::vector<cmh_particles> take_inputs(const cmh_particles *parts, int nbox, cudaStream_t s);
+  // one-buffer mode, after a run's launches are queued: the next staged run's
+  // copies, behind the events that say its buffer is free
+  void queue_pending();
+  void ensure_side();
+  void copy_inputs(const cmh_particles *parts, int nbox, int buf, bool behind_run);
 };
 
 }  // namespace cmh

@@ -205,6 +205,15 @@ cmh_status cmh_plan_run(cmh_plan *plan, const cmh_particles *parts,
  * read_data.c:100-404); nothing there overlaps. */
 cmh_status cmh_plan_prefetch(cmh_plan *plan, const cmh_particles *parts, void *stream);
 
+/* Device buffers for host-resident inputs: 2 (the default) lets
+ * cmh_plan_prefetch copy the next run's inputs while the current run still
+ * reads its own; with 1 (for workspaces that leave no room for a second copy)
+ * the next run's positions are copied into the same buffer once the current
+ * run's ingest has read its positions, and its velocities once the property
+ * sums have read the velocities, so the copies still overlap most of the
+ * run.  Staged copies are dropped.  No reference counterpart. */
+cmh_status cmh_plan_set_input_buffers(cmh_plan *plan, int32_t n);
+
 /* cmh_plan_prefetch for the `nbox` host-resident boxes of a later
  * cmh_plan_run_batch (or cmh_plan_run_batch_status) given the same boxes in
  * the same order: every box's positions are copied before any velocities.

@@ -1,7 +1,7 @@
 """Generate the full-size fixtures: the oracle run once, on the CPU, over
 exactly the workloads that bench.py times.
 
-    python tests/golden/make_fullsize.py [c1 c2 c3 c4]
+    python tests/golden/make_fullsize.py [c1 c2 c3 c4 c5s]
 
 The oracle (oracle/fof_oracle.c) is the CPU restatement of the reference's
 FoF pinned to the reference binaries by tests/test_oracle_pin.py and
@@ -20,7 +20,11 @@ Workloads (the bench's seeds): c1 = synth.config1(seed=1), the 64^3 box
 with FP64 positions; c2 = synth.config2(seed=2), the 256^3 box of the
 headline number; c3 = synth.config3(seed=3), the 50M-particle lightcone
 with a variable linking length; c4 = synth.config4(seed=4), the 64 boxes of
-the batched run (summaries concatenated, with per-box offsets).
+the batched run (summaries concatenated, with per-box offsets); c5s =
+synth.config5(seed=5, scale=1/8), the 1024^3 box's parameters (density,
+clump density, Nphalomin 20) over one eighth of its volume: 134M particles
+in L = 1000 (the full box is drawn on the GPU by the bench and is beyond
+this oracle's memory here).
 """
 from __future__ import annotations
 
@@ -44,6 +48,7 @@ WORKLOADS = {
     "c2": lambda: [synth.config2(seed=2)],
     "c3": lambda: [synth.config3(seed=3)],
     "c4": lambda: synth.config4(seed=4),
+    "c5s": lambda: [synth.config5(seed=5, scale=1 / 8)],
 }
 
 STAT_KEYS = ("n_in", "n_out", "n_images", "n_proc", "n_groups", "n_candidates", "nhalos")

@@ -213,3 +213,47 @@ def test_host_batch_with_prefetch():
             plan.run_batch(cfgs, mpos, hvel)
     finally:
         plan.close()
+
+
+def _shell_box(seed, n=20000):
+    """A periodic box whose particles all lie within Boundarysize of the
+    faces on every axis: about 7 images per particle, far above the plan's
+    first capacity estimate, so the first run overflows and is repeated."""
+    w = synth.make_box(n, 100.0, 40, seed, boundary=10.0)
+    rng = np.random.default_rng(seed)
+    x = (w.pos.astype(np.float64) * 0.09) % 9.0
+    flip = rng.random(x.shape) < 0.5
+    w.pos = np.where(flip, 99.99 - x, x).astype(np.float32)
+    return w
+
+
+def test_one_input_buffer_prefetch():
+    """One input buffer: the next run's copies wait until the current run
+    has read its inputs (positions after ingest, velocities after the sums),
+    in both the eager and the replayed runs; a run that overflows its
+    capacity and repeats gets its own inputs copied again; every catalog
+    matches the oracle."""
+    import torch
+    ws = [_shell_box(501), synth.config2(seed=502, scale=20000 / 256 ** 3)]
+    refs = [cpu.run(w) for w in ws]
+    host = [(torch.from_numpy(w.pos).pin_memory().numpy(),
+             torch.from_numpy(w.vel).pin_memory().numpy()) for w in ws]
+    plan = Plan(FofConfig.from_workload(ws[0]))
+    try:
+        plan.set_input_buffers(1)
+        # box 0 overflows on its first run, with box 1's copies already queued
+        plan.prefetch(*host[0])
+        plan.prefetch(*host[1])
+        assert_same_catalog(plan.run(*host[0], members=True), refs[0])
+        plan.set_config(FofConfig.from_workload(ws[1]))
+        assert_same_catalog(plan.run(*host[1], members=True), refs[1])
+        # a stream of runs of one box: eager, captured, then replays
+        plan.prefetch(*host[1])
+        for i in range(5):
+            if i + 1 < 5:
+                plan.prefetch(*host[1])
+            assert_same_catalog(plan.run(*host[1], members=True), refs[1])
+        with pytest.raises(cmh.CmhError):
+            plan.set_input_buffers(3)
+    finally:
+        plan.close()

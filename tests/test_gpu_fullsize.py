@@ -15,9 +15,10 @@ the C ABI and compares:
   i.e. bit-exact membership of every input particle.
 
 Workloads: the 64^3 box with FP64 positions, the 256^3 box of the headline
-number, the 50M-particle lightcone with a variable linking length, and the
-64 boxes of the batched run (through the batched entry point, and box by
-box for the member sets)."""
+number, the 50M-particle lightcone with a variable linking length, the 64
+boxes of the batched run (through the batched entry point, and box by box
+for the member sets), and the 1024^3 box's parameters over one eighth of
+its volume (134M particles)."""
 import json
 
 import numpy as np
@@ -34,6 +35,7 @@ WORKLOADS = {
     "c2": lambda: [synth.config2(seed=2)],
     "c3": lambda: [synth.config3(seed=3)],
     "c4": lambda: synth.config4(seed=4),
+    "c5s": lambda: [synth.config5(seed=5, scale=1 / 8)],
 }
 _cache = {}
 
@@ -139,3 +141,16 @@ def test_fullsize_batched_boxes_match_oracle():
     for b, w in enumerate(boxes):
         cat = fof(w.pos, w.vel, cfgs[b], members=True)
         check_catalog(cat, fx, b)
+
+
+def test_fullsize_1024_parameters_eighth_volume_match_oracle():
+    """The 1024^3 box's parameters (mean density, clump density, Nphalomin
+    20) over one eighth of its volume: 134M particles in L = 1000, one
+    shot from host arrays, every halo's member set against the oracle."""
+    boxes, fx = workload("c5s")
+    w = boxes[0]
+    cat = fof(w.pos, w.vel, FofConfig.from_workload(w, precision="fp32"), members=True)
+    exp = check_catalog(cat, fx, 0)
+    for k in ("n_in", "n_out", "n_images", "n_proc", "n_groups", "n_candidates"):
+        assert cat.stats[k] == exp[k], (k, cat.stats[k], exp[k])
+    _cache.clear()

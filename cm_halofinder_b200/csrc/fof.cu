@@ -478,60 +478,60 @@ __global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ 
   }
 }
 
-// 1 on the first fine cell of a top cell with more than dense_min fine cells
-// (the first R entries: their scan reads no more).
-__global__ void __launch_bounds__(kT) k_dense_flags(const uint64_t *__restrict__ run_g,
-                                                    const uint16_t *__restrict__ run_box,
-                                                    const BoxDev *__restrict__ boxes,
-                                                    const DevScal *__restrict__ sc,
-                                                    const uint2 *__restrict__ top_range,
-                                                    uint32_t dense_min,
-                                                    uint32_t *__restrict__ flag) {
-  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  const uint32_t R = sc->R;
-  for (int64_t r = gtid(); r < (int64_t)R; r += gstride()) {
-    const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
-    const uint2 tr = top_range[t];
-    flag[r] = (tr.x == (uint32_t)r && tr.y - tr.x > dense_min) ? 1u : 0u;
-  }
-}
-
 // Dense top cells with more fine cells than this are joined by a whole CTA,
 // the others by one warp each.
 constexpr uint32_t kBigTop = 64;
 
-// Slots of the dense top cells (the first nd_cap of them; a dense top cell
-// without a slot is scanned instead, which is slower but exact): the top
-// cell's slot and fine-cell range; the slots of the big ones are listed in
-// `big`.  One thread per top cell's first fine cell.
-__global__ void __launch_bounds__(kT) k_dense_slots(const uint64_t *__restrict__ run_g,
-                                                    const uint16_t *__restrict__ run_box,
-                                                    const BoxDev *__restrict__ boxes,
-                                                    DevScal *sc,
-                                                    const uint2 *__restrict__ top_range,
-                                                    const uint32_t *__restrict__ dflag,
-                                                    const uint32_t *__restrict__ dscan,
-                                                    uint32_t nd_cap,
-                                                    uint32_t *__restrict__ top_slot,
-                                                    uint2 *__restrict__ dense_range,
-                                                    uint32_t *__restrict__ big) {
-  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  const uint32_t R = sc->R;
-  for (int64_t r = gtid(); r < R; r += gstride()) {
-    if (!dflag[r]) continue;
-    const uint32_t slot = dscan[r];
-    if (slot >= nd_cap) continue;
-    const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
-    const uint2 tr = top_range[t];
-    top_slot[t] = slot;
-    dense_range[slot] = tr;
-    if (tr.y - tr.x > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
-  }
+// Warp-aggregated slot from a counter for the lanes with `pick` set: one
+// atomic per warp, the lanes in lane order after the returned base.
+__device__ __forceinline__ uint32_t warp_slot(bool pick, uint32_t *counter) {
+  const uint32_t m = __ballot_sync(0xffffffffu, pick);
+  if (m == 0) return 0u;
+  const int lane = threadIdx.x & 31, first = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == first) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, first);
+  return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
-__global__ void k_clamp_dense(DevScal *sc, uint32_t nd_cap) {
+// Dense top cells (more than dense_min fine cells), one thread per fine
+// cell, acting at each top cell's first: a slot from a counter (the order of
+// the slots does not matter), the top cell's slot and fine-cell range, and
+// the big ones' slots listed in `big`.  Past nd_cap a dense top cell gets no
+// slot and is scanned instead (slower but exact), and the overflow bit asks
+// the plan for more slots next time.
+__global__ void __launch_bounds__(kT) k_dense_pick(const uint64_t *__restrict__ run_g,
+                                                   const uint16_t *__restrict__ run_box,
+                                                   const BoxDev *__restrict__ boxes,
+                                                   DevScal *sc,
+                                                   const uint2 *__restrict__ top_range,
+                                                   uint32_t dense_min, uint32_t nd_cap,
+                                                   uint32_t *__restrict__ top_slot,
+                                                   uint2 *__restrict__ dense_range,
+                                                   uint32_t *__restrict__ big) {
   if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  if (threadIdx.x == 0 && blockIdx.x == 0 && sc->nd > nd_cap) atomicOr(&sc->overflow, 2u);
+  const uint32_t R = sc->R;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r0 = gtid() - lane; r0 < (int64_t)R; r0 += gstride()) {
+    const int64_t r = r0 + lane;
+    bool pick = false;
+    uint64_t t = 0;
+    uint2 tr = make_uint2(0u, 0u);
+    if (r < (int64_t)R) {
+      t = top_of_run(boxes[run_box[r]], run_g[r]);
+      tr = top_range[t];
+      pick = tr.x == (uint32_t)r && tr.y - tr.x > dense_min;
+    }
+    const uint32_t slot = warp_slot(pick, &sc->nd);
+    if (!pick) continue;
+    if (slot < nd_cap) {
+      top_slot[t] = slot;
+      dense_range[slot] = tr;
+      if (tr.y - tr.x > kBigTop) big[atomicAdd(&sc->nbig, 1u)] = slot;
+    } else {
+      atomicOr(&sc->overflow, 2u);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(kT) k_iota(uint32_t *__restrict__ a,
@@ -1290,41 +1290,38 @@ __global__ void __launch_bounds__(kT) k_subsample(
   }
 }
 
-// Candidate flags of the R fine cells: roots with at least Nphalomin
-// members (FOF.c:202).
-__global__ void __launch_bounds__(kT) k_cand_flags(const uint32_t *__restrict__ parent,
-                                                   const uint32_t *__restrict__ count,
-                                                   const uint16_t *__restrict__ run_box,
-                                                   const BoxDev *__restrict__ boxes,
-                                                   const DevScal *__restrict__ sc,
-                                                   uint32_t *__restrict__ flag,
-                                                   unsigned long long *ngroups) {
+// Candidate halos: roots of at least Nphalomin members (FOF.c:202), each
+// given an index from a counter (the catalog is put in head order later, so
+// the candidates' order does not matter); counts the roots (groups).
+__global__ void __launch_bounds__(kT) k_cand_pick(const uint32_t *__restrict__ parent,
+                                                  const uint32_t *__restrict__ count,
+                                                  const uint16_t *__restrict__ run_box,
+                                                  const BoxDev *__restrict__ boxes,
+                                                  DevScal *sc,
+                                                  uint32_t *__restrict__ cand_of_root,
+                                                  uint32_t *__restrict__ cand_root,
+                                                  unsigned long long *ngroups) {
   if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t R = sc->R;
+  const int lane = threadIdx.x & 31;
   unsigned long long roots = 0;
-  // (the scan of the flags reads the first R only)
-  for (int64_t r = gtid(); r < (int64_t)R; r += gstride()) {
-    const bool root = parent[r] == (uint32_t)r;
-    roots += root;
-    flag[r] = (root && !((double)count[r] < boxes[run_box[r]].g.nphalomin)) ? 1u : 0u;
+  for (int64_t r0 = gtid() - lane; r0 < (int64_t)R; r0 += gstride()) {
+    const int64_t r = r0 + lane;
+    bool cand = false;
+    if (r < (int64_t)R) {
+      const bool root = parent[r] == (uint32_t)r;
+      roots += root;
+      cand = root && !((double)count[r] < boxes[run_box[r]].g.nphalomin);
+    }
+    const uint32_t ci = warp_slot(cand, &sc->nc);
+    if (cand) {
+      cand_of_root[r] = ci;
+      cand_root[ci] = (uint32_t)r;
+    }
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) roots += __shfl_down_sync(0xffffffffu, roots, d);
-  if ((threadIdx.x & 31) == 0 && roots) atomicAdd(ngroups, roots);
-}
-
-__global__ void __launch_bounds__(kT) k_cand_list(const uint32_t *__restrict__ flag,
-                                                  const uint32_t *__restrict__ scan,
-                                                  const DevScal *__restrict__ sc,
-                                                  uint32_t *__restrict__ cand_of_root,
-                                                  uint32_t *__restrict__ cand_root) {
-  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  const uint32_t R = sc->R;
-  for (int64_t r = gtid(); r < R; r += gstride()) {
-    if (!flag[r]) continue;
-    cand_of_root[r] = scan[r];
-    cand_root[scan[r]] = (uint32_t)r;
-  }
+  if (lane == 0 && roots) atomicAdd(ngroups, roots);
 }
 
 // Property sums per candidate halo, in double as Output_Halos does
@@ -1395,21 +1392,27 @@ __global__ void __launch_bounds__(kT) k_group_sums(
 }
 
 // Ownership (Checkhalo, FOF.c:394-401): centre of mass by division, kept iff
-// inside [lo, hi) on every axis.  Flags are 0 past the candidate count.
+// inside [lo, hi) on every axis.  An owned candidate is listed with its head
+// as the key of the catalog's sort (from a counter: the sort by head fixes
+// the order).
 template <int NS>
-__global__ void __launch_bounds__(kT) k_owned(const double *__restrict__ sums,
-                                              const uint32_t *__restrict__ cand_root,
-                                              const uint32_t *__restrict__ count,
-                                              const uint16_t *__restrict__ run_box,
-                                              const BoxDev *__restrict__ boxes,
-                                              const DevScal *__restrict__ sc, int64_t cap,
-                                              uint32_t *__restrict__ own) {
+__global__ void __launch_bounds__(kT) k_own_pick(const double *__restrict__ sums,
+                                                 const uint32_t *__restrict__ cand_root,
+                                                 const uint32_t *__restrict__ count,
+                                                 const uint32_t *__restrict__ head,
+                                                 const uint16_t *__restrict__ run_box,
+                                                 const BoxDev *__restrict__ boxes,
+                                                 DevScal *sc, uint32_t *__restrict__ okeys,
+                                                 uint32_t *__restrict__ ovals) {
   if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   const uint32_t nc = sc->nc;
-  for (int64_t c = gtid(); c < cap; c += gstride()) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t c0 = gtid() - lane; c0 < (int64_t)nc; c0 += gstride()) {
+    const int64_t c = c0 + lane;
     bool ok = false;
-    if (c < nc) {
-      const uint32_t root = cand_root[c];
+    uint32_t root = 0;
+    if (c < (int64_t)nc) {
+      root = cand_root[c];
       const Geom &g = boxes[run_box[root]].g;
       const double n = (double)count[root];
       ok = true;
@@ -1419,23 +1422,11 @@ __global__ void __launch_bounds__(kT) k_owned(const double *__restrict__ sums,
         ok &= (com >= g.lo[a]) && (com < g.hi[a]);
       }
     }
-    own[c] = ok ? 1u : 0u;
-  }
-}
-
-__global__ void __launch_bounds__(kT) k_own_list(const uint32_t *__restrict__ own,
-                                                 const uint32_t *__restrict__ own_scan,
-                                                 const uint32_t *__restrict__ cand_root,
-                                                 const uint32_t *__restrict__ head,
-                                                 const DevScal *__restrict__ sc,
-                                                 uint32_t *__restrict__ okeys,
-                                                 uint32_t *__restrict__ ovals) {
-  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  const uint32_t nc = sc->nc;
-  for (int64_t c = gtid(); c < nc; c += gstride()) {
-    if (!own[c]) continue;
-    okeys[own_scan[c]] = head[cand_root[c]];
-    ovals[own_scan[c]] = (uint32_t)c;
+    const uint32_t o = warp_slot(ok, &sc->nh);
+    if (ok) {
+      okeys[o] = head[root];
+      ovals[o] = (uint32_t)c;
+    }
   }
 }
 
@@ -1806,18 +1797,10 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   k_top_ranges<<<rg(k_top_ranges, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
                                  b_top_range.as<uint32_t>());
   CMH_LAUNCHED();
-  k_dense_flags<<<rg(k_dense_flags, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                  b_top_range.as<uint2>(), dense_min,
-                                  b_rtmp1.as<uint32_t>());
-  CMH_LAUNCHED();
-  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nd, scan_tmp, s,
-                     &sc->R);
-  k_clamp_dense<<<1, 32, 0, s>>>(sc, (uint32_t)nd_cap);
-  CMH_LAUNCHED();
-  k_dense_slots<<<rg(k_dense_slots, npc), kT, 0, s>>>(
-      run_g, b_run_box.as<uint16_t>(), boxes, sc, b_top_range.as<uint2>(),
-      b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), (uint32_t)nd_cap,
-      b_top_slot.as<uint32_t>(), b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>());
+  k_dense_pick<<<rg(k_dense_pick, npc), kT, 0, s>>>(
+      run_g, b_run_box.as<uint16_t>(), boxes, sc, b_top_range.as<uint2>(), dense_min,
+      (uint32_t)nd_cap, b_top_slot.as<uint32_t>(), b_dense_range.as<uint2>(),
+      b_dense_big.as<uint32_t>());
   CMH_LAUNCHED();
   k_iota<<<rg(k_iota, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
@@ -1882,14 +1865,9 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
         samp_in, samp_out, samp_seed, samp_closed, b_samp.as<uint8_t>());
     CMH_LAUNCHED();
   }
-  k_cand_flags<<<rg(k_cand_flags, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), b_count.as<uint32_t>(),
-                                 b_run_box.as<uint16_t>(), boxes, sc,
-                                 b_rtmp1.as<uint32_t>(), extra + 0);
-  CMH_LAUNCHED();
-  exclusive_scan_u32(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), npc, &sc->nc, scan_tmp, s,
-                     &sc->R);
-  k_cand_list<<<rg(k_cand_list, npc), kT, 0, s>>>(b_rtmp1.as<uint32_t>(), b_rtmp2.as<uint32_t>(), sc,
-                                b_cand_of_root.as<uint32_t>(), b_cand_root.as<uint32_t>());
+  k_cand_pick<<<rg(k_cand_pick, npc), kT, 0, s>>>(
+      b_parent.as<uint32_t>(), b_count.as<uint32_t>(), b_run_box.as<uint16_t>(), boxes, sc,
+      b_cand_of_root.as<uint32_t>(), b_cand_root.as<uint32_t>(), extra + 0);
   CMH_LAUNCHED();
   mark(4);
 
@@ -1917,18 +1895,14 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   mark(5);
   if (vel_wait) record_external(ev_vel_free, s);  // nor their velocities
 #define CMH_OWNED(NSV)                                                                          \
-  k_owned<NSV><<<rg(k_owned<NSV>, ncc), kT, 0, s>>>(b_sums.as<double>(), b_cand_root.as<uint32_t>(),              \
-                                 b_count.as<uint32_t>(), b_run_box.as<uint16_t>(), boxes, sc, \
-                                 ncc, b_own.as<uint32_t>())
+  k_own_pick<NSV><<<rg(k_own_pick<NSV>, ncc), kT, 0, s>>>(                                      \
+      b_sums.as<double>(), b_cand_root.as<uint32_t>(), b_count.as<uint32_t>(),                  \
+      b_head.as<uint32_t>(), b_run_box.as<uint16_t>(), boxes, sc, b_okeys.as<uint32_t>(),       \
+      b_ovals.as<uint32_t>())
   if (NS == 6) CMH_OWNED(6);
   else if (NS == 12) CMH_OWNED(12);
   else CMH_OWNED(18);
 #undef CMH_OWNED
-  CMH_LAUNCHED();
-  exclusive_scan_u32(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(), ncc, &sc->nh, scan_tmp, s);
-  k_own_list<<<rg(k_own_list, ncc), kT, 0, s>>>(b_own.as<uint32_t>(), b_own_scan.as<uint32_t>(),
-                               b_cand_root.as<uint32_t>(), b_head.as<uint32_t>(), sc,
-                               b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>());
   CMH_LAUNCHED();
   radix_sort_u32_u32(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), b_okeys_alt.as<uint32_t>(),
                      b_ovals_alt.as<uint32_t>(), ncc, &sc->nh, bits_for((uint64_t)npc),
@@ -2060,8 +2034,6 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
   b_cand_root.ensure(ncc * 4);
   b_sums.ensure(ncc * 18 * 8);
   b_warn.ensure(ncc * 4);
-  b_own.ensure(ncc * 4);
-  b_own_scan.ensure(ncc * 4);
   b_okeys.ensure(ncc * 4);
   b_ovals.ensure(ncc * 4);
   b_okeys_alt.ensure(ncc * 4);

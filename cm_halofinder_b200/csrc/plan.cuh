@@ -101,7 +101,7 @@ struct Plan : public cmh_plan {
   DevBuf b_run_start, b_run_box, b_top_range, b_top_slot, b_rtmp1, b_rtmp2;
   DevBuf b_rows, b_dense_range, b_dense_big;
   DevBuf b_parent, b_count, b_head, b_cand_of_root, b_cand_root, b_sums, b_warn;
-  DevBuf b_own, b_own_scan, b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
+  DevBuf b_okeys, b_ovals, b_okeys_alt, b_ovals_alt;
   DevBuf b_props, b_head_out, b_cat_of_cand, b_member, b_member_proc, b_member_pos;
   DevBuf in_pos[2], in_vel[2];  // device copies of host-resident particles
   DevBuf b_samp;          // per input particle: 0, 1 (kept, in a halo), 2 (kept, outside)
@@ -112,8 +112,8 @@ struct Plan : public cmh_plan {
                      &b_keys, &b_keys_alt, &b_vals, &b_vals_alt, &b_ppos, &b_spos, &b_svl,
                      &b_run_start, &b_run_box, &b_top_range, &b_top_slot,
                      &b_rtmp1, &b_rtmp2, &b_rows, &b_dense_range, &b_dense_big, &b_parent, &b_count,
-                     &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn, &b_own,
-                     &b_own_scan, &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
+                     &b_head, &b_cand_of_root, &b_cand_root, &b_sums, &b_warn,
+                     &b_okeys, &b_ovals, &b_okeys_alt, &b_ovals_alt, &b_props,
                      &b_head_out, &b_cat_of_cand, &b_member, &b_member_proc, &b_member_pos,
                      &in_pos[0], &in_vel[0], &in_pos[1], &in_vel[1], &b_samp};
     for (DevBuf *b : all) f(*b);

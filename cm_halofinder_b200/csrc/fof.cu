@@ -399,8 +399,17 @@ __global__ void __launch_bounds__(kT) k_gather_flags(const uint32_t *__restrict_
   }
 }
 
+__device__ __forceinline__ uint64_t top_of_run(const BoxDev &bx, uint64_t pg) {
+  const Geom &g = bx.g;
+  const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
+  return bx.top_base +
+         ((uint64_t)div_k(gz, g) * g.T[1] + (uint64_t)div_k(gy, g)) * g.T[0] + div_k(gx, g);
+}
+
 // Run of every processed particle, and per run its first particle, packed
-// fine cell and box.
+// fine cell, box and initial parent (itself); the range of runs of every
+// occupied top cell ([first, last + 1), written where the top cell changes
+// between neighbouring particles; top_range starts zeroed).
 template <class PT>
 __global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ cells,
                                              const uint32_t *__restrict__ flag,
@@ -411,21 +420,36 @@ __global__ void __launch_bounds__(kT) k_runs(const uint64_t *__restrict__ cells,
                                              uint32_t *__restrict__ run_of,
                                              uint32_t *__restrict__ run_start,
                                              uint64_t *__restrict__ run_g,
-                                             uint16_t *__restrict__ run_box) {
+                                             uint16_t *__restrict__ run_box,
+                                             uint32_t *__restrict__ parent,
+                                             uint32_t *__restrict__ top_range) {
   if (sc->failed) return;  // a sort of this run gave up: its order is not valid
   __shared__ uint64_t s_base[kMaxBoxes];
   load_bases(boxes, nbox, s_base, false);
   const int64_t np = sc->np;
   const uint32_t R = sc->R;
+  auto box_of = [&](int64_t i) {
+    return nbox > 1 ? box_search(s_base, nbox, (uint64_t)spos[i].src) : 0;
+  };
   for (int64_t i = gtid(); i < np; i += gstride()) {
     const uint32_t f = flag[i];
     const uint32_t rid = run_scan[i] + f - 1u;
+    const bool last = i == np - 1 || flag[i + 1] != 0u;
     run_of[i] = rid;
+    if (!f && !last) continue;
+    const uint64_t c = cells[i];
+    const int b = box_of(i);
+    const uint64_t t = top_of_run(boxes[b], c);
     if (f) {
       run_start[rid] = (uint32_t)i;
-      run_g[rid] = cells[i];
-      run_box[rid] = (uint16_t)(nbox > 1 ? box_search(s_base, nbox, (uint64_t)spos[i].src) : 0);
+      run_g[rid] = c;
+      run_box[rid] = (uint16_t)b;
+      parent[rid] = rid;
+      if (i == 0 || top_of_run(boxes[box_of(i - 1)], cells[i - 1]) != t)
+        top_range[2 * t] = rid;
     }
+    if (last && (i == np - 1 || top_of_run(boxes[box_of(i + 1)], cells[i + 1]) != t))
+      top_range[2 * t + 1] = rid + 1u;
     if (i == np - 1) run_start[R] = (uint32_t)np;
   }
 }
@@ -453,28 +477,6 @@ __global__ void __launch_bounds__(kT) k_varlink_recs(const SPos<PT> *__restrict_
       v.lsq = ref_cell_linksq(g, v.rkey);
     }
     svl[i] = v;
-  }
-}
-
-__device__ __forceinline__ uint64_t top_of_run(const BoxDev &bx, uint64_t pg) {
-  const Geom &g = bx.g;
-  const int gx = (int)(pg & kM21), gy = (int)((pg >> 21) & kM21), gz = (int)(pg >> 42);
-  return bx.top_base +
-         ((uint64_t)div_k(gz, g) * g.T[1] + (uint64_t)div_k(gy, g)) * g.T[0] + div_k(gx, g);
-}
-
-__global__ void __launch_bounds__(kT) k_top_ranges(const uint64_t *__restrict__ run_g,
-                                                   const uint16_t *__restrict__ run_box,
-                                                   const BoxDev *__restrict__ boxes,
-                                                   const DevScal *__restrict__ sc,
-                                                   uint32_t *__restrict__ top_range) {
-  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  const uint32_t R = sc->R;
-  for (int64_t r = gtid(); r < R; r += gstride()) {
-    const uint64_t t = top_of_run(boxes[run_box[r]], run_g[r]);
-    if (r == 0 || top_of_run(boxes[run_box[r - 1]], run_g[r - 1]) != t) top_range[2 * t] = (uint32_t)r;
-    if (r == R - 1 || top_of_run(boxes[run_box[r + 1]], run_g[r + 1]) != t)
-      top_range[2 * t + 1] = (uint32_t)(r + 1);
   }
 }
 
@@ -534,12 +536,6 @@ __global__ void __launch_bounds__(kT) k_dense_pick(const uint64_t *__restrict__ 
   }
 }
 
-__global__ void __launch_bounds__(kT) k_iota(uint32_t *__restrict__ a,
-                                             const DevScal *__restrict__ sc) {
-  if (sc->failed) return;  // a sort of this run gave up: its order is not valid
-  const uint32_t R = sc->R;
-  for (int64_t r = gtid(); r < R; r += gstride()) a[r] = (uint32_t)r;
-}
 
 // ---------------------------------------------------------------------------
 // Befriending.
@@ -1776,10 +1772,12 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
       b_keys.as<uint64_t>(), flag, sc);
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s, &sc->np);
+  CMH_CUDA(cudaMemsetAsync(b_top_range.p, 0, n_top * 8, s));
   k_runs<PT><<<rg(k_runs<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan,
                                                b_spos.as<SPos<PT>>(), boxes, nbox, sc, run_of,
                                                b_run_start.as<uint32_t>(), run_g,
-                                               b_run_box.as<uint16_t>());
+                                               b_run_box.as<uint16_t>(), b_parent.as<uint32_t>(),
+                                               b_top_range.as<uint32_t>());
   CMH_LAUNCHED();
   if (varlink) {
     if (fp32)
@@ -1792,17 +1790,11 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                                   b_svl.as<VLRec64>());
     CMH_LAUNCHED();
   }
-  CMH_CUDA(cudaMemsetAsync(b_top_range.p, 0, n_top * 8, s));
   CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, s));
-  k_top_ranges<<<rg(k_top_ranges, npc), kT, 0, s>>>(run_g, b_run_box.as<uint16_t>(), boxes, sc,
-                                 b_top_range.as<uint32_t>());
-  CMH_LAUNCHED();
   k_dense_pick<<<rg(k_dense_pick, npc), kT, 0, s>>>(
       run_g, b_run_box.as<uint16_t>(), boxes, sc, b_top_range.as<uint2>(), dense_min,
       (uint32_t)nd_cap, b_top_slot.as<uint32_t>(), b_dense_range.as<uint2>(),
       b_dense_big.as<uint32_t>());
-  CMH_LAUNCHED();
-  k_iota<<<rg(k_iota, npc), kT, 0, s>>>(b_parent.as<uint32_t>(), sc);
   CMH_LAUNCHED();
   mark(2);
   // ---- befriending: dense top cells inside (CTA each), fast path, queue,

@@ -2361,7 +2361,9 @@ void Plan::copy_inputs(const cmh_particles *parts, int nbox, int b, bool behind_
 }
 
 void Plan::queue_pending() {
-  if (input_buffers != 1 || staged.empty() || !staged.front().pending) return;
+  // (a run on device-resident particles records no free events: what is
+  // staged waits for the next run on host inputs)
+  if (input_buffers != 1 || !vel_wait || staged.empty() || !staged.front().pending) return;
   Staged &f = staged.front();
   std::vector<size_t> opos, ovel;
   size_t tpos, tvel;

@@ -253,6 +253,15 @@ def test_one_input_buffer_prefetch():
             if i + 1 < 5:
                 plan.prefetch(*host[1])
             assert_same_catalog(plan.run(*host[1], members=True), refs[1])
+        # a run on device-resident particles between them leaves the staged
+        # copies alone (it records no free events to wait for)
+        dpos = torch.from_numpy(ws[1].pos).cuda()
+        dvel = torch.from_numpy(ws[1].vel).cuda()
+        plan.prefetch(*host[1])
+        plan.prefetch(*host[1])
+        assert_same_catalog(plan.run(dpos, dvel, members=True), refs[1])
+        for _ in range(2):
+            assert_same_catalog(plan.run(*host[1], members=True), refs[1])
         with pytest.raises(cmh.CmhError):
             plan.set_input_buffers(3)
     finally:

@@ -330,6 +330,16 @@ def run_ours(args):
                           "eager step after the timed region",
                 "stage_gbs": {k: round(sb[k] / (stages[k] * 1e-3) / 1e9, 1)
                               for k in sb if stages.get(k, 0) > 0}}
+    if stages.get("befriend", 0) > 0:
+        # the befriending stage's work rates beside its GB/s: particle-pair
+        # tests (about 9 FP32 operations each) and candidate fine-cell pairs
+        # (most of them ended by a union-find check, no pair test)
+        sec = stages["befriend"] * 1e-3
+        roofline["befriend_rates"] = {
+            "pair_tests_per_s": round(st["n_pair_tests"] / sec, 1),
+            "pair_test_gflops_fp32": round(9 * st["n_pair_tests"] / sec / 1e9, 2),
+            "cell_pairs_per_s": round(st["n_cell_pairs"] / sec, 1),
+            "root_skips_per_s": round(st["n_root_skips"] / sec, 1)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

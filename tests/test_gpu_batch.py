@@ -266,3 +266,47 @@ def test_one_input_buffer_prefetch():
             plan.set_input_buffers(3)
     finally:
         plan.close()
+
+
+def test_dense_slots_beyond_capacity_then_grown():
+    """Every top cell of two or more fine cells dense (dense_min 1, large top
+    cells): the first run has far more dense top cells than slots, leaves
+    the rest to the sparse path and asks for more slots; every run, before
+    and after the growth, eager and replayed, matches the oracle."""
+    import torch
+    w = synth.config2(seed=511, scale=200000 / 256 ** 3)
+    ref = cpu.run(w)
+    pos = torch.from_numpy(w.pos).cuda()
+    vel = torch.from_numpy(w.vel).cuda()
+    plan = Plan(FofConfig.from_workload(w))
+    try:
+        plan.set_tuning({"cell_scale": 2.0, "dense_min": 1})
+        cats = [plan.run(pos, vel, members=True) for _ in range(3)]
+        assert cats[0].stats["n_dense_tops"] > 200000 // 1024 + 1024
+        for cat in cats:
+            assert_same_catalog(cat, ref)
+    finally:
+        plan.close()
+
+
+def test_one_input_buffer_batch_prefetch():
+    """prefetch_batch with one input buffer: the next batch's copies wait
+    until the current batch has read its inputs."""
+    import torch
+    boxes = _boxes(4, 13)
+    refs = [cpu.run(w) for w in boxes]
+    cfgs = [FofConfig.from_workload(w) for w in boxes]
+    hpos = [torch.from_numpy(w.pos).pin_memory().numpy() for w in boxes]
+    hvel = [torch.from_numpy(w.vel).pin_memory().numpy() for w in boxes]
+    plan = Plan(cfgs[0])
+    try:
+        plan.set_input_buffers(1)
+        plan.prefetch_batch(hpos, hvel)
+        for i in range(4):
+            if i + 1 < 4:
+                plan.prefetch_batch(hpos, hvel)
+            cats = plan.run_batch(cfgs, hpos, hvel)
+            for cat, ref in zip(cats, refs):
+                assert_same_catalog(cat, ref, check_member=False)
+    finally:
+        plan.close()

@@ -112,6 +112,12 @@ Plan::~Plan() {
     if (g) cudaGraphExecDestroy(g);
   if (side_stream) cudaStreamSynchronize(side_stream);
   if (cap_stream) cudaStreamDestroy(cap_stream);
+  if (bf_stream) {
+    cudaStreamSynchronize(bf_stream);
+    cudaStreamDestroy(bf_stream);
+  }
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
   if (side_stream) cudaStreamDestroy(side_stream);
   if (ev_side_start) cudaEventDestroy(ev_side_start);
   if (ev_pos_free) cudaEventDestroy(ev_pos_free);

@@ -744,7 +744,9 @@ __device__ __forceinline__ uint32_t bit_span(int lo, int hi) {
 
 // Dense top cells: the fine-cell pairs inside a top cell are joined with a
 // union-find in shared memory, near pairs before far ones; then every fine
-// cell's global parent is set to its local root.  Links that cross the top
+// cell is joined to its local root in the global union-find (a
+// compare-and-swap of its own parent when nothing else has hooked it, a
+// union otherwise: the sparse kernel runs at the same time).  Links that cross the top
 // cell's faces are left to the global passes.  The occupied fine cells of
 // the top cell are first marked in bit rows (bit x of rows[z k + y]), so a
 // cell visits only the occupied cells of its forward window, a row at a
@@ -849,7 +851,13 @@ __device__ __forceinline__ void dense_top(uint32_t slot, uint32_t *lpar, uint32_
     }
     sync();
   }
-  for (uint32_t i = tid; i < n; i += nt) parent[f + i] = f + lfind(lpar, i);
+  // joined to its local root through the global union-find: the sparse
+  // kernel runs at the same time and may have hooked a cell of this top cell
+  for (uint32_t i = tid; i < n; i += nt) {
+    const uint32_t r = f + lfind(lpar, i);
+    if (r != f + i && atomicCAS(parent + f + i, f + i, r) != f + i)
+      uf_union(parent, f + i, r, ctr, g.union_cap);
+  }
   // rows and prefixes stay for the warp path, which looks up this top
   // cell's fine cells from its neighbours
   uint32_t *gr = grows + (uint64_t)slot * 2 * kk;
@@ -1797,8 +1805,9 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
       b_dense_big.as<uint32_t>());
   CMH_LAUNCHED();
   mark(2);
-  // ---- befriending: dense top cells inside (CTA each), fast path, queue,
-  // warp path near then far ----
+  // ---- befriending: dense top cells inside (CTA each) on a second stream
+  // while the sparse fast path runs (both join cells through the lock-free
+  // union-find), then the queued cells' warp path, near then far ----
   uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense slots
   const int dwpc = dense_warps_per_cta(k3all);
   const uint32_t kk = (uint32_t)rows_per_top(k3all);
@@ -1809,17 +1818,22 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     constexpr bool FP = decltype(fp32_tag)::value;
     constexpr bool VL = decltype(vl_tag)::value;
     const VLRec<FP> *svl = VL ? b_svl.as<VLRec<FP>>() : nullptr;
-    k_befriend_dense<PT, FP, VL><<<gd, 32 * dwpc, dsm, s>>>(
+    // dense top cells on a second stream, beside the sparse cells
+    CMH_CUDA(cudaEventRecord(ev_fork, s));
+    CMH_CUDA(cudaStreamWaitEvent(bf_stream, ev_fork, 0));
+    k_befriend_dense<PT, FP, VL><<<gd, 32 * dwpc, dsm, bf_stream>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         run_g, b_dense_range.as<uint2>(), b_dense_big.as<uint32_t>(), sc, (uint32_t)nd_cap,
         b_rows.as<uint32_t>(), kk, b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), c,
         (uint32_t)dense_words(k3all));
     CMH_LAUNCHED();
+    CMH_CUDA(cudaEventRecord(ev_join, bf_stream));
     k_befriend_simple<PT, FP, VL><<<rg(k_befriend_simple<PT, FP, VL>, npc), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), b_run_start.as<uint32_t>(), run_g,
         sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
         b_spos.as<SPos<PT>>(), svl, b_parent.as<uint32_t>(), queue, c);
     CMH_LAUNCHED();
+    CMH_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
     k_befriend<PT, FP, VL, 0><<<rg(k_befriend<PT, FP, VL, 0>, npc * 32), kT, 0, s>>>(
         boxes, b_run_box.as<uint16_t>(), k3all, b_run_start.as<uint32_t>(),
         run_g, queue, sc, b_top_range.as<uint2>(), b_top_slot.as<uint32_t>(),
@@ -1934,6 +1948,11 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
 }
 
 void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
+  if (!bf_stream) {
+    CMH_CUDA(cudaStreamCreateWithFlags(&bf_stream, cudaStreamNonBlocking));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  }
   const int nbox = (int)specs.size();
   if (nbox < 1 || nbox > kMaxBoxes) fail(CMH_ERR_INVALID_ARGUMENT, "1 to 1024 boxes per run");
   boxes_host.resize(nbox);

@@ -56,6 +56,8 @@ struct Plan : public cmh_plan {
   bool launches_per_run_graph_ok = false;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t bf_stream = nullptr;  // the dense top cells' kernel, beside the sparse one
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t stage_ev[7] = {};  // boundaries between the eight stages
   // the recorded graphs of the last two run shapes (two, so that runs that
   // alternate between the two host-input buffers both replay)

@@ -1744,10 +1744,14 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                                       nimg);
     CMH_LAUNCHED();
   }
-  exclusive_scan_u32(keep, keep_scan, n, &sc->kept_total,
-                     scan_tmp, s);
-  exclusive_scan_u32(nimg, img_scan, n, &sc->img_total,
-                     scan_tmp, s);
+  // the keep and image scans side by side (the image scan on the second
+  // stream, with its own scratch)
+  CMH_CUDA(cudaEventRecord(ev_fork, s));
+  CMH_CUDA(cudaStreamWaitEvent(bf_stream, ev_fork, 0));
+  exclusive_scan_u32(nimg, img_scan, n, &sc->img_total, scan_tmp2, bf_stream);
+  CMH_CUDA(cudaEventRecord(ev_join, bf_stream));
+  exclusive_scan_u32(keep, keep_scan, n, &sc->kept_total, scan_tmp, s);
+  CMH_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
   k_box_totals<<<1, 32, 0, s>>>(boxes, nbox, n, keep_scan,
                                 img_scan, sc, boxd, (uint32_t)npc);
   CMH_LAUNCHED();
@@ -2082,6 +2086,7 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
       need += 2 * m;
     }
     scan_tmp.ensure((size_t)(need + 16) * sizeof(uint32_t));
+    scan_tmp2.ensure((size_t)(need + 16) * sizeof(uint32_t));
     sort_tmp.ensure(radix_sort_scratch(std::max(npc, ncc)));
   }
 }

@@ -98,7 +98,7 @@ struct Plan : public cmh_plan {
   const uint64_t *samp_ids = nullptr;
 
   // workspace
-  DevBuf scal, ctr, scan_tmp, sort_tmp, ltab_dev, b_boxes, b_boxd;
+  DevBuf scal, ctr, scan_tmp, scan_tmp2, sort_tmp, ltab_dev, b_boxes, b_boxd;
   DevBuf b_keys, b_keys_alt, b_vals, b_vals_alt, b_ppos, b_spos, b_svl;
   DevBuf b_run_start, b_run_box, b_top_range, b_top_slot, b_rtmp1, b_rtmp2;
   DevBuf b_rows, b_dense_range, b_dense_big;
@@ -110,7 +110,7 @@ struct Plan : public cmh_plan {
 
   // every workspace buffer, for release and for the graph signature
   template <class F> void each_buf(F f) {
-    DevBuf *all[] = {&scal, &ctr, &scan_tmp, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd,
+    DevBuf *all[] = {&scal, &ctr, &scan_tmp, &scan_tmp2, &sort_tmp, &ltab_dev, &b_boxes, &b_boxd,
                      &b_keys, &b_keys_alt, &b_vals, &b_vals_alt, &b_ppos, &b_spos, &b_svl,
                      &b_run_start, &b_run_box, &b_top_range, &b_top_slot,
                      &b_rtmp1, &b_rtmp2, &b_rows, &b_dense_range, &b_dense_big, &b_parent, &b_count,

@@ -118,6 +118,8 @@ Plan::~Plan() {
   }
   if (ev_fork) cudaEventDestroy(ev_fork);
   if (ev_join) cudaEventDestroy(ev_join);
+  for (cudaEvent_t e : {ev_cleared, ev_emitted, ev_cleared2})
+    if (e) cudaEventDestroy(e);
   if (side_stream) cudaStreamDestroy(side_stream);
   if (ev_side_start) cudaEventDestroy(ev_side_start);
   if (ev_pos_free) cudaEventDestroy(ev_pos_free);

@@ -1750,6 +1750,21 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_CUDA(cudaStreamWaitEvent(bf_stream, ev_fork, 0));
   exclusive_scan_u32(nimg, img_scan, n, &sc->img_total, scan_tmp2, bf_stream);
   CMH_CUDA(cudaEventRecord(ev_join, bf_stream));
+  // then, on that stream, the clearing of the later stages' tables, which
+  // overlaps the ingest and the sort (their first users wait for it)
+  const int NS = 6 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
+  CMH_CUDA(cudaMemsetAsync(b_top_range.p, 0, n_top * 8, bf_stream));
+  CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, bf_stream));
+  CMH_CUDA(cudaMemsetAsync(b_cand_of_root.p, 0xff, npc * 4, bf_stream));
+  CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, bf_stream));
+  CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, (size_t)ncc * 4, bf_stream));
+  CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, (size_t)ncc * 4, bf_stream));
+  if (want_member && n > 0) {
+    CMH_CUDA(cudaMemsetAsync(b_member.p, 0xff, (size_t)n * 8, bf_stream));
+    CMH_CUDA(cudaMemsetAsync(b_member_proc.p, 0xff, (size_t)n * 4, bf_stream));
+    CMH_CUDA(cudaMemsetAsync(b_member_pos.p, 0, (size_t)n * 12, bf_stream));
+  }
+  CMH_CUDA(cudaEventRecord(ev_cleared, bf_stream));
   exclusive_scan_u32(keep, keep_scan, n, &sc->kept_total, scan_tmp, s);
   CMH_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
   k_box_totals<<<1, 32, 0, s>>>(boxes, nbox, n, keep_scan,
@@ -1763,6 +1778,13 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_LAUNCHED();
   }
   mark(0);
+  // the ingest's flag arrays become the group counts and heads: cleared on
+  // the second stream once the emission has read them
+  CMH_CUDA(cudaEventRecord(ev_emitted, s));
+  CMH_CUDA(cudaStreamWaitEvent(bf_stream, ev_emitted, 0));
+  CMH_CUDA(cudaMemsetAsync(b_count.p, 0, npc * 4, bf_stream));
+  CMH_CUDA(cudaMemsetAsync(b_head.p, 0xff, npc * 4, bf_stream));
+  CMH_CUDA(cudaEventRecord(ev_cleared2, bf_stream));
   // host inputs: their positions are read no more (a next run's may be
   // copied into their buffer)
   if (vel_wait) record_external(ev_pos_free, s);
@@ -1784,7 +1806,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
       b_keys.as<uint64_t>(), flag, sc);
   CMH_LAUNCHED();
   exclusive_scan_u32(flag, run_scan, npc, &sc->R, scan_tmp, s, &sc->np);
-  CMH_CUDA(cudaMemsetAsync(b_top_range.p, 0, n_top * 8, s));
+  CMH_CUDA(cudaStreamWaitEvent(s, ev_cleared, 0));  // top ranges and slots cleared
   k_runs<PT><<<rg(k_runs<PT>, npc), kT, 0, s>>>(b_keys.as<uint64_t>(), flag, run_scan,
                                                b_spos.as<SPos<PT>>(), boxes, nbox, sc, run_of,
                                                b_run_start.as<uint32_t>(), run_g,
@@ -1802,7 +1824,6 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
                                                   b_svl.as<VLRec64>());
     CMH_LAUNCHED();
   }
-  CMH_CUDA(cudaMemsetAsync(b_top_slot.p, 0xff, n_top * 4, s));
   k_dense_pick<<<rg(k_dense_pick, npc), kT, 0, s>>>(
       run_g, b_run_box.as<uint16_t>(), boxes, sc, b_top_range.as<uint2>(), dense_min,
       (uint32_t)nd_cap, b_top_slot.as<uint32_t>(), b_dense_range.as<uint2>(),
@@ -1860,9 +1881,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   mark(3);
 
   // ---- groups, candidates ----
-  CMH_CUDA(cudaMemsetAsync(b_count.p, 0, npc * 4, s));
-  CMH_CUDA(cudaMemsetAsync(b_head.p, 0xff, npc * 4, s));
-  CMH_CUDA(cudaMemsetAsync(b_cand_of_root.p, 0xff, npc * 4, s));
+  CMH_CUDA(cudaStreamWaitEvent(s, ev_cleared2, 0));  // counts and heads cleared
   k_group_count<<<rg(k_group_count, npc), kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
                                   b_vals.as<uint32_t>(), sc, b_count.as<uint32_t>(),
                                   b_head.as<uint32_t>());
@@ -1888,9 +1907,6 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
     CMH_CUDA(cudaStreamWaitEvent(s, ev_vel_ready,
                                  capturing(s) ? cudaEventWaitExternal : cudaEventWaitDefault));
   }
-  const int NS = 6 + ((props & 1) ? 6 : 0) + ((props & 2) ? 6 : 0);
-  CMH_CUDA(cudaMemsetAsync(b_sums.p, 0, (size_t)ncc * NS * 8, s));
-  CMH_CUDA(cudaMemsetAsync(b_warn.p, 0, (size_t)ncc * 4, s));
 #define CMH_SUMS(NSV)                                                                         \
   k_group_sums<PT, NSV><<<rg(k_group_sums<PT, NSV>, npc), kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),  \
                                           b_cand_of_root.as<uint32_t>(),                      \
@@ -1917,7 +1933,6 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   radix_sort_u32_u32(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), b_okeys_alt.as<uint32_t>(),
                      b_ovals_alt.as<uint32_t>(), ncc, &sc->nh, bits_for((uint64_t)npc),
                      sort_tmp, &sc->failed, s, SortWaits{spin_cap, 0xffffffffu});
-  CMH_CUDA(cudaMemsetAsync(b_cat_of_cand.p, 0xff, (size_t)ncc * 4, s));
 #define CMH_CATALOG(NSV)                                                                        \
   k_catalog<NSV><<<rg(k_catalog<NSV>, ncc), kT, 0, s>>>(b_okeys.as<uint32_t>(), b_ovals.as<uint32_t>(), sc,          \
                                    b_sums.as<double>(), b_cand_root.as<uint32_t>(),             \
@@ -1934,9 +1949,6 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   CMH_LAUNCHED();
   mark(6);
   if (want_member && n > 0) {
-    CMH_CUDA(cudaMemsetAsync(b_member.p, 0xff, (size_t)n * 8, s));
-    CMH_CUDA(cudaMemsetAsync(b_member_proc.p, 0xff, (size_t)n * 4, s));
-    CMH_CUDA(cudaMemsetAsync(b_member_pos.p, 0, (size_t)n * 12, s));
     k_member<PT><<<rg(k_member<PT>, npc), kT, 0, s>>>(run_of, b_parent.as<uint32_t>(),
                                    b_cand_of_root.as<uint32_t>(), b_cat_of_cand.as<uint32_t>(),
                                    b_spos.as<SPos<PT>>(), sc, b_member.as<unsigned long long>());
@@ -1956,6 +1968,9 @@ void Plan::prepare(const std::vector<BoxSpec> &specs, bool want_member) {
     CMH_CUDA(cudaStreamCreateWithFlags(&bf_stream, cudaStreamNonBlocking));
     CMH_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     CMH_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_cleared, cudaEventDisableTiming));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_emitted, cudaEventDisableTiming));
+    CMH_CUDA(cudaEventCreateWithFlags(&ev_cleared2, cudaEventDisableTiming));
   }
   const int nbox = (int)specs.size();
   if (nbox < 1 || nbox > kMaxBoxes) fail(CMH_ERR_INVALID_ARGUMENT, "1 to 1024 boxes per run");

@@ -58,6 +58,7 @@ struct Plan : public cmh_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t bf_stream = nullptr;  // the dense top cells' kernel, beside the sparse one
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_cleared = nullptr, ev_emitted = nullptr, ev_cleared2 = nullptr;
   cudaEvent_t stage_ev[7] = {};  // boundaries between the eight stages
   // the recorded graphs of the last two run shapes (two, so that runs that
   // alternate between the two host-input buffers both replay)

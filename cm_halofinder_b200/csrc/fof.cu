@@ -1833,7 +1833,7 @@ void Plan::issue(bool want_member, cudaStream_t s, bool timed) {
   // ---- befriending: dense top cells inside (CTA each) on a second stream
   // while the sparse fast path runs (both join cells through the lock-free
   // union-find), then the queued cells' warp path, near then far ----
-  uint32_t *queue = b_rtmp1.as<uint32_t>();  // free again after the dense slots
+  uint32_t *queue = b_rtmp1.as<uint32_t>();  // the keep scan's, free since the emission
   const int dwpc = dense_warps_per_cta(k3all);
   const uint32_t kk = (uint32_t)rows_per_top(k3all);
   const size_t dsm = (size_t)dwpc * dense_words(k3all) * sizeof(uint32_t);
